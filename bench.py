@@ -1,0 +1,346 @@
+"""Benchmark of the B200 hash groupby-aggregate engine.
+
+Workload (the 100M-row single groupby): 100,000,000 rows; int64 key drawn
+uniformly from 1,000,000 distinct random 64-bit values; v1 int64 uniform in
+[-1e9, 1e9], v2 float64 normal(0,1), v3 float32 lognormal(0,1); an independent
+10% Bernoulli null mask per value column; SUM/COUNT/MIN/MAX/MEAN on each value
+column; seed 1.  Synthetic data, generated on the device.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Prints one JSON line (rank 0).  `value` is rows/s of the whole aggregate() call
+with inputs resident in HBM (device-timed with CUDA events, max over ranks);
+`e2e` is the same call through the public API with pinned host inputs copied
+in and results copied out inside the timed region.  `--impl reference` times
+the CPU restatement of the reference algorithm (oracle/) on the host cores on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_ROWS = 100_000_000
+N_DISTINCT = 1_000_000
+SEED = 1
+NULL_FRAC = 0.10
+AGG_NAMES = ["sum", "count", "min", "max", "mean"]
+METRIC = "groupby rows/s (100M rows, 1M groups, 3 value cols, sum/count/min/max/mean)"
+CPU_SAMPLE_ROWS = 8_000_000
+
+
+def algorithmic_bytes(n_rows: int, n_groups: int) -> tuple[float, float]:
+    """Bytes the groupby must move at least once: every input column and mask
+    read once, every output column and mask written once."""
+    mask = ((n_rows + 31) // 32) * 4
+    inp = n_rows * (8 + 8 + 8 + 4) + 3 * mask
+    gmask = ((n_groups + 31) // 32) * 4
+    # keys 8; per value col: sum, count(4), min, max, mean(8) + masks for sum/min/max/mean
+    out = n_groups * 8 + n_groups * (8 + 4 + 8 + 8 + 8) * 2 + n_groups * (4 + 4 + 4 + 4 + 8) + 3 * 4 * gmask
+    return float(inp), float(out)
+
+
+def make_inputs_host(n: int, seed: int = SEED):
+    rng = np.random.default_rng(seed)
+    distinct = np.unique(rng.integers(-2**63, 2**63 - 1, N_DISTINCT, dtype=np.int64))
+    key = distinct[rng.integers(0, distinct.size, n)]
+    v1 = rng.integers(-10**9, 10**9, n, endpoint=True).astype(np.int64)
+    v2 = rng.normal(size=n)
+    v3 = rng.lognormal(size=n).astype(np.float32)
+    masks = [rng.random(n) >= NULL_FRAC for _ in range(3)]
+    return key, [v1, v2, v3], masks
+
+
+def make_inputs_device(n: int, seed: int, device):
+    import torch
+    from cudf_b200.column import pack_mask
+    rng = np.random.default_rng(seed)
+    distinct = torch.from_numpy(np.unique(rng.integers(-2**63, 2**63 - 1, N_DISTINCT, dtype=np.int64))).to(device)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    idx = torch.randint(0, distinct.numel(), (n,), device=device, generator=g)
+    key = distinct[idx]
+    del idx
+    v1 = torch.randint(-10**9, 10**9 + 1, (n,), device=device, generator=g, dtype=torch.int64)
+    v2 = torch.randn(n, device=device, generator=g, dtype=torch.float64)
+    v3 = torch.empty(n, device=device, dtype=torch.float32).log_normal_(0.0, 1.0, generator=g)
+    masks = [pack_mask(torch.rand(n, device=device, generator=g) >= NULL_FRAC) for _ in range(3)]
+    return key, [v1, v2, v3], masks
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def cpu_reference(n_sample: int, threads: int):
+    """The oracle (CPU restatement of the reference algorithm) on a sample."""
+    from oracle import oracle as O
+    key, vals, masks = make_inputs_host(n_sample)
+    kinds = [O.SUM, O.COUNT_VALID, O.MIN, O.MAX, O.MEAN]
+    kc = O.HostColumn(O.INT64, key)
+    reqs = [(O.HostColumn(O.INT64, vals[0], masks[0]), kinds),
+            (O.HostColumn(O.FLOAT64, vals[1], masks[1]), kinds),
+            (O.HostColumn(O.FLOAT32, vals[2], masks[2]), kinds)]
+    O.groupby([kc], reqs, nthreads=threads)  # warm
+    t = time.perf_counter()
+    O.groupby([kc], reqs, nthreads=threads)
+    return n_sample / (time.perf_counter() - t)
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    n_sample = CPU_SAMPLE_ROWS
+    vals = []
+    for _ in range(max(1, args.steps)):
+        vals.append(cpu_reference(n_sample, threads))
+    v = float(np.median(vals))
+    line = {"metric": METRIC, "value": v, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": N_ROWS / v * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64/f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "groupby 100M rows, int64 key over 1M distinct values, v1 int64, "
+                                   "v2 f64, v3 f32, 10% nulls, sum/count/min/max/mean", "rows": N_ROWS,
+                       "groups": N_DISTINCT, "parallelism": f"replicas{world}"},
+            "cpu_baseline": {"value": v, "unit": "rows/s", "cores": threads, "kind": "port",
+                             "sample": f"first {n_sample} rows of the same generator (seed 1), "
+                                       f"oracle/gb_oracle.c with {threads} threads"},
+            "e2e": {"value": v, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_engine(args):
+    import torch
+    world, rank, local = dist_setup()
+    import cudf_b200 as cb
+    from cudf_b200 import aggregation as agg
+    from cudf_b200.types import TypeId
+
+    dev = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(dev)
+    n = args.rows
+    key, vals, masks = make_inputs_device(n, SEED + rank, dev)
+    torch.cuda.synchronize()
+    aggs = [agg.sum(), agg.count(), agg.min(), agg.max(), agg.mean()]
+    kcol = cb.Column(TypeId.INT64, key)
+    vcols = [cb.Column(TypeId.INT64, vals[0], masks[0]), cb.Column(TypeId.FLOAT64, vals[1], masks[1]),
+             cb.Column(TypeId.FLOAT32, vals[2], masks[2])]
+    gb = cb.GroupBy(cb.Table([kcol]))
+    gb.set_tuning(**json.loads(args.tuning)) if args.tuning else None
+    gb.set_profile(True)
+    reqs = [cb.GroupByRequest(c, aggs) for c in vcols]
+    stream = torch.cuda.current_stream()
+
+    def step():
+        return gb.aggregate(reqs)
+
+    for _ in range(args.warmup):
+        out = step()
+    del out
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kernel_ms = []
+    groups = 0
+    launches = 0
+    with ClockSampler(dev.index) as clk:
+        torch.cuda.synchronize()
+        start.record(stream)
+        for _ in range(args.steps):
+            uk, res = step()
+            st = gb.stats()
+            kernel_ms.append(st["agg_kernel_ms"])
+            launches += st["kernels"]
+            groups = uk.num_rows()
+        end.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    del uk, res
+
+    # ---- e2e through the public API from pinned host buffers ----
+    hkey = key.cpu().pin_memory()
+    hvals = [v.cpu().pin_memory() for v in vals]
+    hmasks = [m.cpu().pin_memory() for m in masks]
+    dkey = torch.empty_like(key)
+    dvals = [torch.empty_like(v) for v in vals]
+    dmasks = [torch.empty_like(m) for m in masks]
+    del key, vals, masks, kcol, vcols, reqs, gb
+    ek = cb.Column(TypeId.INT64, dkey)
+    ev = [cb.Column(TypeId.INT64, dvals[0], dmasks[0]), cb.Column(TypeId.FLOAT64, dvals[1], dmasks[1]),
+          cb.Column(TypeId.FLOAT32, dvals[2], dmasks[2])]
+    ereqs = [cb.GroupByRequest(c, aggs) for c in ev]
+    h2d = sum(t.numel() * t.element_size() for t in [hkey, *hvals, *hmasks])
+    d2h = 0
+
+    def e2e_step():
+        nonlocal d2h
+        dkey.copy_(hkey, non_blocking=True)
+        for d, h in zip(dvals + dmasks, hvals + hmasks):
+            d.copy_(h, non_blocking=True)
+        g2 = cb.GroupBy(cb.Table([ek]))
+        uk2, res2 = g2.aggregate(ereqs)
+        outs = [c.values() for c in uk2.columns] + [c.values() for t in res2 for c in t.columns]
+        outs += [c.mask for t in res2 for c in t.columns if c.mask is not None]
+        host = [o.cpu() for o in outs]
+        d2h = sum(h.numel() * h.element_size() for h in host)
+        return host
+
+    e2e_step()
+    torch.cuda.synchronize()
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_steps = max(1, min(args.steps, 3))
+    e_start.record(stream)
+    for _ in range(e_steps):
+        e2e_step()
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    e_ms = e_start.elapsed_time(e_end) / e_steps
+    if world > 1:
+        t = torch.tensor([e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e_ms = float(t.item())
+
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        peak = float(peaks.get("hbm_gbs", 6650.0))
+        peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+        inp, outb = algorithmic_bytes(n, groups)
+        kmean = float(np.mean(kernel_ms)) if kernel_ms else float("nan")
+        achieved = inp / (kmean * 1e-3) / 1e9
+        value = world * n / (ms * 1e-3)
+        line = {
+            "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64/f64/f32", "data": "synthetic",
+            "config": {"workload": "groupby 100M rows, int64 key over 1M distinct values, v1 int64, "
+                                   "v2 f64, v3 f32, 10% nulls, sum/count/min/max/mean",
+                       "rows": n, "groups": groups, "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "l2": "inputs (2.84 GB) larger than L2 (126 MB); no flush needed"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "k_aggregate",
+                         "kernel_ms": kmean, "peak_source": peak_src,
+                         "whole_call_frac": (inp + outb) / (ms * 1e-3) / 1e9 / peak},
+            "e2e": {"value": world * n / (e_ms * 1e-3), "unit": "rows/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        if not args.no_cpu_baseline and world == 1:
+            threads = os.cpu_count() or 1
+            v = cpu_reference(args.cpu_sample, threads)
+            line["cpu_baseline"] = {"value": v, "unit": "rows/s", "cores": threads, "kind": "port",
+                                    "sample": f"first {args.cpu_sample} rows of the same generator "
+                                              f"(seed 1) through oracle/gb_oracle.c, {threads} threads"}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--rows", type=int, default=N_ROWS)
+    ap.add_argument("--tuning", default="")
+    ap.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE_ROWS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_engine(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,12 @@
+"""cudf_b200 -- a B200-native (sm_100a) hash groupby-aggregate engine that is a
+drop-in for libcudf's ``cudf::groupby::groupby(keys, null_policy).aggregate``
+path.  The compute path is the CUDA library built by ``cudf_b200.build``; there
+is no CPU fallback."""
+from . import aggregation
+from .column import Column, Table
+from .groupby import GroupBy, GroupByRequest
+from .types import Kind, NullPolicy, Sorted, TypeId
+
+__all__ = ["aggregation", "Column", "Table", "GroupBy", "GroupByRequest", "Kind", "NullPolicy",
+           "Sorted", "TypeId"]
+__version__ = "0.1.0"

@@ -1,0 +1,653 @@
+// gb_engine.cu -- host orchestration of the hash groupby: planning, table
+// sizing from a key sample, launches, overflow retry and compaction.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gb_engine.h"
+#include "gb_kernels.cuh"
+
+namespace gb {
+
+// ---------------------------------------------------------------------------
+// type system (cpp/include/cudf/detail/aggregation/aggregation.hpp:1168-1290)
+int type_width(int t)
+{
+  switch (t) {
+    case T_INT8: case T_UINT8: case T_BOOL8: return 1;
+    case T_INT16: case T_UINT16: return 2;
+    case T_INT32: case T_UINT32: case T_FLOAT32: case T_TS_D: case T_DUR_D: return 4;
+    case T_INT64: case T_UINT64: case T_FLOAT64: case T_TS_S: case T_TS_MS: case T_TS_US:
+    case T_TS_NS: case T_DUR_S: case T_DUR_MS: case T_DUR_US: case T_DUR_NS: return 8;
+    default: return 0;
+  }
+}
+static bool is_ts(int t) { return t >= T_TS_D && t <= T_TS_NS; }
+static bool is_dur(int t) { return t >= T_DUR_D && t <= T_DUR_NS; }
+static uint8_t type_cat(int t)
+{
+  if (t == T_FLOAT32) return CAT_F32;
+  if (t == T_FLOAT64) return CAT_F64;
+  if (t == T_BOOL8) return CAT_BOOL;
+  if (t >= T_UINT8 && t <= T_UINT64) return CAT_UNSIGNED;
+  return CAT_SIGNED;
+}
+
+bool valid_agg(int t, int k)
+{
+  if (type_width(t) == 0) return false;
+  bool numeric = !is_ts(t) && !is_dur(t);
+  switch (k) {
+    case K_MIN: case K_MAX: case K_COUNT_VALID: case K_COUNT_ALL: case K_ARGMIN: case K_ARGMAX: return true;
+    case K_SUM: case K_MEAN: return numeric || is_dur(t);
+    case K_PRODUCT: case K_SUM_OF_SQUARES: case K_VARIANCE: case K_STD: return numeric;
+    default: return false;
+  }
+}
+
+int target_type(int t, int k)
+{
+  switch (k) {
+    case K_COUNT_VALID: case K_COUNT_ALL: case K_ARGMIN: case K_ARGMAX: return T_INT32;
+    case K_MIN: case K_MAX: return t;
+    case K_VARIANCE: case K_STD: return T_FLOAT64;
+    case K_MEAN: return is_dur(t) ? t : T_FLOAT64;
+    case K_SUM: case K_PRODUCT: case K_SUM_OF_SQUARES:
+      return (t == T_FLOAT32 || t == T_FLOAT64 || is_dur(t)) ? t : T_INT64;
+    default: return T_EMPTY;
+  }
+}
+
+// ---------------------------------------------------------------------------
+static void ck(cudaError_t e, const char* what)
+{
+  if (e == cudaSuccess) return;
+  cudaGetLastError();
+  throw Error(e == cudaErrorMemoryAllocation ? ERR_ALLOC : ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+static void* default_alloc(void*, size_t bytes, void* stream)
+{
+  static std::once_flag once;
+  std::call_once(once, [] {
+    // keep freed blocks cached in the pool: repeated calls then allocate in O(1)
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+  });
+  void* p = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMallocAsync(&p, bytes, (cudaStream_t)stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+static void default_free(void*, void* p, size_t, void* stream)
+{
+  if (p) cudaFreeAsync(p, (cudaStream_t)stream);
+}
+Allocator default_allocator() { return Allocator{default_alloc, default_free, nullptr}; }
+
+// Scratch buffers of one call, returned to the allocator on scope exit.
+struct Scratch {
+  Allocator A;
+  cudaStream_t s;
+  struct Buf { void* p; size_t n; };
+  std::vector<Buf> bufs;
+  Scratch(const Allocator& a, cudaStream_t st) : A(a), s(st) {}
+  void* get(size_t n)
+  {
+    void* p = A.allocate(A.ctx, n, (void*)s);
+    if (!p) throw Error(ERR_ALLOC, "device allocation of " + std::to_string(n) + " bytes failed");
+    bufs.push_back({p, n});
+    return p;
+  }
+  void put(void* p)
+  {
+    for (size_t i = 0; i < bufs.size(); ++i)
+      if (bufs[i].p == p) {
+        A.deallocate(A.ctx, p, bufs[i].n, (void*)s);
+        bufs.erase(bufs.begin() + i);
+        return;
+      }
+  }
+  ~Scratch()
+  {
+    for (auto& b : bufs) A.deallocate(A.ctx, b.p, b.n, (void*)s);
+  }
+};
+
+void Result::release()
+{
+  auto fr = [&](void* p, size_t n) {
+    if (p && alloc.deallocate) alloc.deallocate(alloc.ctx, p, n, (void*)stream);
+  };
+  for (auto& c : keys) { fr(c.data, c.data_bytes); fr(c.mask, c.mask_bytes); }
+  for (auto& r : results)
+    for (auto& c : r) { fr(c.data, c.data_bytes); fr(c.mask, c.mask_bytes); }
+  keys.clear();
+  results.clear();
+}
+
+struct DevInfo {
+  int sms = 148;
+  int smem_optin = 227 * 1024;
+};
+static DevInfo dev_info()
+{
+  static std::mutex mu;
+  static DevInfo cache[64];
+  static bool have[64] = {};
+  int dev = 0;
+  ck(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> g(mu);
+  if (dev < 64 && !have[dev]) {
+    cudaDeviceGetAttribute(&cache[dev].sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&cache[dev].smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    have[dev] = true;
+  }
+  return cache[dev < 64 ? dev : 0];
+}
+
+static uint64_t next_pow2(uint64_t x)
+{
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+// ---------------------------------------------------------------------------
+// planning
+void build_plan(const std::vector<Column>& keys, int null_policy, const std::vector<Request>& reqs,
+                Plan& P, std::vector<int>& out_types)
+{
+  std::memset(&P, 0, sizeof(P));
+  if (keys.empty()) throw Error(ERR_LOGIC, "groupby needs at least one key column");
+  if (keys.size() > (size_t)kMaxKeyCols) throw Error(ERR_UNSUPPORTED, "too many key columns");
+  int64_t n = keys[0].size;
+  for (auto& k : keys) {
+    if (k.size != n) throw Error(ERR_LOGIC, "Size mismatch between key columns.");
+    if (type_width(k.type_id) == 0) throw Error(ERR_UNSUPPORTED, "unsupported key column type");
+  }
+  // cpp/src/groupby/groupby.cu:208-212
+  for (auto& r : reqs)
+    if (r.values.size != n) throw Error(ERR_LOGIC, "Size mismatch between request values and groupby keys.");
+  // cpp/src/groupby/groupby.cu:174-190
+  for (auto& r : reqs)
+    for (auto& a : r.aggs)
+      if (!valid_agg(r.values.type_id, a.kind)) throw Error(ERR_LOGIC, "Invalid type/aggregation combination.");
+  if (n >= (int64_t)0xFFFFFFF0ll) throw Error(ERR_UNSUPPORTED, "more than 2^32-16 rows in one groupby");
+
+  P.num_rows = n;
+  P.include_nulls = null_policy == 1;
+  P.num_keys = (int)keys.size();
+  // key packing, first-fit decreasing: value bits never straddle a word, null
+  // flags (INCLUDE only) are single bits; word 0 holds 64 bits, word 1 at most
+  // 63 so that its top bit stays clear (the empty-slot marker of 2-word keys)
+  struct Item { int bits, key; bool null_flag; };
+  std::vector<Item> items;
+  for (int k = 0; k < P.num_keys; ++k) {
+    KeyCol& c = P.keys[k];
+    c.data = keys[k].data;
+    c.mask = keys[k].mask;
+    c.offset = keys[k].offset;
+    c.type_id = keys[k].type_id;
+    c.width = (uint8_t)type_width(c.type_id);
+    c.cat = type_cat(c.type_id);
+    if (c.mask) P.any_key_nullable = 1;
+    items.push_back({8 * c.width, k, false});
+    if (c.mask && P.include_nulls) {
+      items.push_back({1, k, true});
+      c.has_null_bit = 1;
+    }
+  }
+  std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) { return a.bits > b.bits; });
+  int used[2] = {0, 0};
+  const int room[2] = {64, 63};
+  int words = 1;
+  for (auto& it : items) {
+    int w = 0;
+    while (w < 2 && used[w] + it.bits > room[w]) ++w;
+    if (w == 2) throw Error(ERR_UNSUPPORTED, "key rows wider than 127 packed bits are not supported");
+    KeyCol& c = P.keys[it.key];
+    if (it.null_flag) { c.null_word = (uint8_t)w; c.null_shift = (uint8_t)used[w]; }
+    else { c.word = (uint8_t)w; c.shift = (uint8_t)used[w]; }
+    used[w] += it.bits;
+    words = std::max(words, w + 1);
+  }
+  P.key_words = words;
+
+  // value columns: one entry per distinct (column view, ddof of VAR/STD)
+  struct VKey { Column c; int ddof; };
+  std::vector<VKey> vk;
+  std::vector<std::vector<int>> need(0);
+  auto find_col = [&](const Column& c, int ddof) {
+    for (size_t i = 0; i < vk.size(); ++i)
+      if (vk[i].c.data == c.data && vk[i].c.mask == c.mask && vk[i].c.offset == c.offset &&
+          vk[i].c.type_id == c.type_id && vk[i].ddof == ddof)
+        return (int)i;
+    vk.push_back({c, ddof});
+    return (int)vk.size() - 1;
+  };
+  // per request/agg: column index
+  std::vector<std::vector<int>> colof(reqs.size());
+  for (size_t r = 0; r < reqs.size(); ++r)
+    for (auto& a : reqs[r].aggs) {
+      bool var = a.kind == K_VARIANCE || a.kind == K_STD;
+      colof[r].push_back(find_col(reqs[r].values, var ? a.ddof : -1));
+    }
+  if (vk.size() > (size_t)kMaxValCols) throw Error(ERR_UNSUPPORTED, "too many distinct value columns");
+  P.num_vals = (int)vk.size();
+
+  // which accumulator ops each column needs
+  std::vector<std::vector<uint8_t>> ops(vk.size());
+  std::vector<bool> need_nulls(vk.size(), false), need_m2(vk.size(), false);
+  auto add = [&](int v, uint8_t op) {
+    if (std::find(ops[v].begin(), ops[v].end(), op) == ops[v].end()) ops[v].push_back(op);
+  };
+  for (size_t r = 0; r < reqs.size(); ++r)
+    for (size_t j = 0; j < reqs[r].aggs.size(); ++j) {
+      int v = colof[r][j];
+      const Column& c = vk[v].c;
+      int t = c.type_id, w = type_width(t);
+      uint8_t cat = type_cat(t);
+      bool fl = cat == CAT_F32 || cat == CAT_F64;
+      int k = reqs[r].aggs[j].kind;
+      if (c.mask && k != K_COUNT_ALL) need_nulls[v] = true;
+      auto sum_op = [&]() -> uint8_t {
+        if (cat == CAT_F32) return OP_SUM_F32;
+        if (cat == CAT_F64) return OP_SUM_F64;
+        if (is_dur(t) && w == 4) return OP_SUM_I32;
+        return OP_SUM_I64;
+      };
+      switch (k) {
+        case K_SUM: case K_MEAN: add(v, sum_op()); break;
+        case K_VARIANCE: case K_STD: add(v, sum_op()); need_m2[v] = true; break;
+        case K_MIN: add(v, w == 8 ? OP_MIN_U64 : OP_MIN_U32); break;
+        case K_MAX: add(v, w == 8 ? OP_MAX_U64 : OP_MAX_U32); break;
+        case K_SUM_OF_SQUARES: add(v, cat == CAT_F32 ? OP_SQ_F32 : cat == CAT_F64 ? OP_SQ_F64 : OP_SQ_I64); break;
+        case K_PRODUCT: add(v, cat == CAT_F32 ? OP_PROD_F32 : cat == CAT_F64 ? OP_PROD_F64 : OP_PROD_I64); break;
+        case K_ARGMIN: add(v, w == 8 ? OP_ARGMIN_R64 : OP_ARGMIN_P32); break;
+        case K_ARGMAX: add(v, w == 8 ? OP_ARGMAX_R64 : OP_ARGMAX_P32); break;
+        default: break;
+      }
+      (void)fl;
+    }
+
+  // slot layout: key words | rows u32 | null counters u32 | 4-byte accs | 8-byte accs
+  auto op_size = [](uint8_t op) {
+    switch (op) {
+      case OP_SUM_I32: case OP_SUM_F32: case OP_MIN_U32: case OP_MAX_U32: case OP_SQ_F32:
+      case OP_PROD_F32: return 4;
+      default: return 8;
+    }
+  };
+  int off = 8 * P.key_words;
+  P.rows_off = off;
+  off += 4;
+  for (size_t v = 0; v < vk.size(); ++v) {
+    ValCol& c = P.vals[v];
+    c.data = vk[v].c.data;
+    c.mask = vk[v].c.mask;
+    c.offset = vk[v].c.offset;
+    c.type_id = vk[v].c.type_id;
+    c.width = (uint8_t)type_width(c.type_id);
+    c.cat = type_cat(c.type_id);
+    c.ddof = vk[v].ddof < 0 ? 1 : vk[v].ddof;
+    c.nulls_off = -1;
+    c.sum_off = -1;
+    c.m2_off = -1;
+    if (need_nulls[v]) { c.nulls_off = (int16_t)off; off += 4; }
+  }
+  // accumulators grouped per column, 4-byte ones first within the slot
+  std::vector<std::pair<int, int>> acc_off;  // (col, op) -> offset resolved below
+  int na = 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1) off = (off + 7) & ~7;
+    for (size_t v = 0; v < vk.size(); ++v)
+      for (uint8_t op : ops[v]) {
+        if ((op_size(op) == 4) != (pass == 0)) continue;
+        if (na >= kMaxAccs) throw Error(ERR_UNSUPPORTED, "too many aggregations in one call");
+        P.accs[na].op = op;
+        P.accs[na].col = (uint8_t)v;
+        P.accs[na].off = (uint16_t)off;
+        off += op_size(op);
+        ++na;
+      }
+  }
+  for (size_t v = 0; v < vk.size(); ++v)
+    if (need_m2[v]) {
+      P.vals[v].m2_off = (int16_t)off;
+      off += 8;
+      P.need_second_pass = 1;
+    }
+  P.num_accs = na;
+  P.slot_bytes = (off + 15) & ~15;
+  if (P.slot_bytes > kMaxSlotBytes) throw Error(ERR_UNSUPPORTED, "too many aggregations in one call");
+  // reorder accs by column so each column owns a contiguous range
+  std::stable_sort(P.accs, P.accs + na, [](const Acc& a, const Acc& b) { return a.col < b.col; });
+  for (size_t v = 0; v < vk.size(); ++v) {
+    ValCol& c = P.vals[v];
+    c.acc_begin = c.acc_end = 0;
+    bool first = true;
+    for (int a = 0; a < na; ++a)
+      if (P.accs[a].col == v) {
+        if (first) { c.acc_begin = (int16_t)a; first = false; }
+        c.acc_end = (int16_t)(a + 1);
+        uint8_t op = P.accs[a].op;
+        if (op == OP_SUM_I64 || op == OP_SUM_I32 || op == OP_SUM_F32 || op == OP_SUM_F64) c.sum_off = (int16_t)P.accs[a].off;
+      }
+  }
+  auto acc_for = [&](int v, uint8_t op) -> int16_t {
+    for (int a = 0; a < na; ++a)
+      if (P.accs[a].col == v && P.accs[a].op == op) return (int16_t)P.accs[a].off;
+    return -1;
+  };
+
+  // outputs in request order
+  out_types.clear();
+  int no = 0;
+  for (size_t r = 0; r < reqs.size(); ++r)
+    for (size_t j = 0; j < reqs[r].aggs.size(); ++j) {
+      if (no >= kMaxOutputs) throw Error(ERR_UNSUPPORTED, "too many aggregations in one call");
+      int v = colof[r][j];
+      const ValCol& c = P.vals[v];
+      OutSpec& o = P.outs[no++];
+      o.kind = reqs[r].aggs[j].kind;
+      o.col = v;
+      o.out_type = target_type(c.type_id, o.kind);
+      o.out_width = (uint8_t)type_width(o.out_type);
+      o.ddof = reqs[r].aggs[j].ddof;
+      bool has_nulls = c.mask != nullptr;
+      int w = c.width;
+      switch (o.kind) {
+        case K_COUNT_VALID: case K_COUNT_ALL: o.nullable = 0; o.acc_off = -1; break;
+        case K_SUM: case K_MEAN: o.nullable = has_nulls; o.acc_off = c.sum_off; break;
+        case K_VARIANCE: case K_STD: o.nullable = 1; o.acc_off = c.m2_off; break;
+        case K_MIN: o.nullable = has_nulls; o.acc_off = acc_for(v, w == 8 ? OP_MIN_U64 : OP_MIN_U32); break;
+        case K_MAX: o.nullable = has_nulls; o.acc_off = acc_for(v, w == 8 ? OP_MAX_U64 : OP_MAX_U32); break;
+        case K_SUM_OF_SQUARES: o.nullable = has_nulls;
+          o.acc_off = acc_for(v, c.cat == CAT_F32 ? OP_SQ_F32 : c.cat == CAT_F64 ? OP_SQ_F64 : OP_SQ_I64); break;
+        case K_PRODUCT: o.nullable = has_nulls;
+          o.acc_off = acc_for(v, c.cat == CAT_F32 ? OP_PROD_F32 : c.cat == CAT_F64 ? OP_PROD_F64 : OP_PROD_I64); break;
+        case K_ARGMIN: o.nullable = has_nulls; o.acc_off = acc_for(v, w == 8 ? OP_ARGMIN_R64 : OP_ARGMIN_P32); break;
+        case K_ARGMAX: o.nullable = has_nulls; o.acc_off = acc_for(v, w == 8 ? OP_ARGMAX_R64 : OP_ARGMAX_P32); break;
+        default: break;
+      }
+      out_types.push_back(o.out_type);
+    }
+  P.num_outs = no;
+}
+
+static void build_template(const Plan& P, SlotTemplate& t)
+{
+  std::memset(&t, 0, sizeof(t));
+  uint8_t* b = (uint8_t*)t.w;
+  std::memset(b, 0xFF, 8 * P.key_words);
+  for (int a = 0; a < P.num_accs; ++a) {
+    uint8_t* p = b + P.accs[a].off;
+    switch (P.accs[a].op) {
+      case OP_MIN_U32: std::memset(p, 0xFF, 4); break;
+      case OP_MIN_U64: case OP_ARGMIN_P32: case OP_ARGMIN_R64: case OP_ARGMAX_R64: std::memset(p, 0xFF, 8); break;
+      case OP_PROD_I64: { int64_t one = 1; std::memcpy(p, &one, 8); break; }
+      case OP_PROD_F32: { float one = 1.0f; std::memcpy(p, &one, 4); break; }
+      case OP_PROD_F64: { double one = 1.0; std::memcpy(p, &one, 8); break; }
+      default: break;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+namespace {
+thread_local uint32_t* t_pinned = nullptr;
+thread_local cudaEvent_t t_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+cudaEvent_t* events()
+{
+  if (!t_ev[0])
+    for (auto& e : t_ev) ck(cudaEventCreate(&e), "cudaEventCreate");
+  return t_ev;
+}
+uint32_t* pinned()
+{
+  if (!t_pinned) ck(cudaMallocHost((void**)&t_pinned, 4096), "cudaMallocHost");
+  return t_pinned;
+}
+
+int grid_for(const void* kernel, int block, size_t smem, int bps_cap)
+{
+  DevInfo d = dev_info();
+  int bps = 0;
+  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, block, smem), "occupancy");
+  if (bps < 1) bps = 1;
+  if (bps_cap > 0) bps = std::min(bps, bps_cap);
+  return d.sms * bps;
+}
+
+OutColumn make_out(const Allocator& A, cudaStream_t s, int type_id, int64_t rows, bool nullable)
+{
+  OutColumn c;
+  c.type_id = type_id;
+  c.size = rows;
+  c.data_bytes = (size_t)std::max<int64_t>(rows, 1) * type_width(type_id);
+  c.data = A.allocate(A.ctx, c.data_bytes, (void*)s);
+  if (!c.data) throw Error(ERR_ALLOC, "device allocation of an output column failed");
+  if (nullable) {
+    c.mask_bytes = (size_t)((std::max<int64_t>(rows, 1) + 511) / 512) * 64;
+    c.mask = (uint32_t*)A.allocate(A.ctx, c.mask_bytes, (void*)s);
+    if (!c.mask) throw Error(ERR_ALLOC, "device allocation of an output mask failed");
+    ck(cudaMemsetAsync(c.mask, 0, c.mask_bytes, s), "memset mask");
+  }
+  return c;
+}
+}  // namespace
+
+Result aggregate(const std::vector<Column>& keys, int null_policy, const std::vector<Request>& reqs,
+                 cudaStream_t stream, const Allocator& alloc, const Options& opt, Stats* stats)
+{
+  Plan P;
+  std::vector<int> out_types;
+  build_plan(keys, null_policy, reqs, P, out_types);
+  Stats st;
+  Result R;
+  R.alloc = alloc;
+  R.stream = stream;
+  const int64_t n = P.num_rows;
+
+  auto empty_result = [&]() {
+    R.num_groups = 0;
+    for (auto& k : keys) R.keys.push_back(make_out(alloc, stream, k.type_id, 0, k.mask != nullptr));
+    int j = 0;
+    for (auto& r : reqs) {
+      std::vector<OutColumn> cols;
+      for (size_t a = 0; a < r.aggs.size(); ++a, ++j)
+        cols.push_back(make_out(alloc, stream, out_types[j], 0, P.outs[j].nullable));
+      R.results.push_back(cols);
+    }
+    return R;
+  };
+  // cpp/src/groupby/groupby.cu:216 -- empty input gives empty outputs
+  if (n == 0) {
+    if (stats) *stats = st;
+    return empty_result();
+  }
+
+  Scratch S(alloc, stream);
+  unsigned int* counters = (unsigned int*)S.get(4096);
+  ck(cudaMemsetAsync(counters, 0, 4096, stream), "memset counters");
+  uint32_t* host = pinned();
+  DevInfo dev = dev_info();
+
+  // ---- group-count estimate ----
+  int64_t est;
+  if (opt.groups_hint >= 0) {
+    est = std::max<int64_t>(1, opt.groups_hint);
+  } else if (n <= 65536) {
+    est = n;
+  } else {
+    const int64_t nsamp = std::min<int64_t>(n, 1 << 18);
+    uint64_t scap = next_pow2((uint64_t)(2 * nsamp));
+    size_t sbytes = (scap + 1) * 32;
+    uint8_t* ST = (uint8_t*)S.get(sbytes);
+    SlotTemplate t;
+    std::memset(&t, 0, sizeof(t));
+    std::memset(&t, 0xFF, 16);
+    k_init_slots<<<dev.sms * 4, 256, 0, stream>>>(ST, (int64_t)scap + 1, 32, t);
+    TableRef SR{ST, scap - 1, 32, P.key_words, counters + 16};
+    k_sample<<<dev.sms * 4, 256, 0, stream>>>(P, SR, nsamp);
+    k_sample_stats<<<dev.sms * 4, 256, 0, stream>>>(P, SR);
+    st.kernels += 3;
+    ck(cudaGetLastError(), "sample launch");
+    ck(cudaMemcpyAsync(host, counters + 16, 16 * 4, cudaMemcpyDeviceToHost, stream), "sample d2h");
+    ck(cudaStreamSynchronize(stream), "sample sync");
+    S.put(ST);
+    double d = host[4], f1 = host[5], f2 = host[6], m = host[3];
+    if (nsamp >= n) est = (int64_t)d;
+    else {
+      // bias-corrected Chao1 on the sample; scaled up when the sample saw
+      // mostly singletons (high cardinality)
+      double c1 = d + f1 * (f1 - 1) / (2 * (f2 + 1));
+      if (m > 0 && f1 > 0.9 * m) c1 = std::max(c1, d * (double)n / m);
+      est = (int64_t)std::min<double>((double)n, std::max(d, c1));
+    }
+    est = std::max<int64_t>(est, 1);
+  }
+  st.est_groups = est;
+
+  // ---- mode and table size ----
+  int scap = 0, sfill = 0;
+  {
+    int sb = std::min(opt.smem_bytes, dev.smem_optin - 1024);
+    if (sb > 0 && P.slot_bytes <= sb) {
+      scap = 1;
+      while ((int64_t)scap * 2 * P.slot_bytes <= sb) scap *= 2;
+      sfill = std::max(1, (int)(scap * opt.smem_fill));
+    }
+  }
+  int64_t smem_max = opt.smem_max_groups >= 0 ? opt.smem_max_groups : 2 * (int64_t)sfill;
+  bool use_smem = scap >= 64 && est <= smem_max;
+  if (opt.force_mode == 0) use_smem = false;
+  if (opt.force_mode == 1 && scap >= 16) use_smem = true;
+  st.mode = use_smem ? 1 : 0;
+
+  uint64_t cap = next_pow2((uint64_t)std::max<double>(1024.0, std::ceil((double)est / opt.load_factor)));
+  cap = std::min<uint64_t>(cap, next_pow2((uint64_t)(2 * n + 2)));
+  cap = std::max<uint64_t>(cap, 1024);
+  SlotTemplate tmpl;
+  build_template(P, tmpl);
+
+  uint8_t* T = nullptr;
+  TableRef G{};
+  for (int attempt = 0;; ++attempt) {
+    size_t tbytes = (size_t)(cap + 1) * P.slot_bytes;
+    T = (uint8_t*)S.get(tbytes);
+    k_init_slots<<<dev.sms * 8, 256, 0, stream>>>(T, (int64_t)cap + 1, P.slot_bytes, tmpl);
+    ck(cudaMemsetAsync(counters, 0, 16, stream), "memset counters");
+    G = TableRef{T, cap - 1, P.slot_bytes, P.key_words, counters};
+    int block = opt.block;
+    if (opt.profile) ck(cudaEventRecord(events()[0], stream), "event");
+    if (use_smem) {
+      size_t sm = (size_t)scap * P.slot_bytes;
+      ck(cudaFuncSetAttribute(k_aggregate<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), "smem attr");
+      int grid = grid_for((const void*)k_aggregate<true>, block, sm, opt.blocks_per_sm);
+      grid = (int)std::min<int64_t>(grid, (n + block - 1) / block);
+      k_aggregate<true><<<grid, block, sm, stream>>>(P, G, scap, sfill, tmpl);
+    } else {
+      int grid = grid_for((const void*)k_aggregate<false>, block, 0, opt.blocks_per_sm);
+      grid = (int)std::min<int64_t>(grid, (n + block - 1) / block);
+      k_aggregate<false><<<grid, block, 0, stream>>>(P, G, 1, 0, tmpl);
+    }
+    if (opt.profile) ck(cudaEventRecord(events()[1], stream), "event");
+    k_finish_count<<<1, 1, 0, stream>>>(P, G);
+    st.kernels += 3;
+    ck(cudaGetLastError(), "aggregate launch");
+    ck(cudaMemcpyAsync(host, counters, 8, cudaMemcpyDeviceToHost, stream), "count d2h");
+    ck(cudaStreamSynchronize(stream), "aggregate sync");
+    if (opt.profile) {
+      float ms = 0;
+      ck(cudaEventElapsedTime(&ms, events()[0], events()[1]), "event time");
+      st.agg_kernel_ms += ms;
+    }
+    if (host[1] == 0) break;
+    // table overflow: the kernel stopped inserting; redo with a larger table
+    if (attempt >= 6) throw Error(ERR_CUDA, "hash table overflow");
+    S.put(T);
+    cap *= 4;
+    ++st.retries;
+  }
+  st.capacity = (int64_t)cap;
+  const int64_t G_n = host[0];
+  R.num_groups = G_n;
+
+  if (P.need_second_pass) {
+    int grid = grid_for((const void*)k_var_pass, 256, 0, 0);
+    k_var_pass<<<grid, 256, 0, stream>>>(P, G);
+    ++st.kernels;
+    ck(cudaGetLastError(), "variance pass launch");
+  }
+
+  // ---- outputs ----
+  try {
+  OutPtrs O;
+  std::memset(&O, 0, sizeof(O));
+  for (int k = 0; k < P.num_keys; ++k) {
+    R.keys.push_back(make_out(alloc, stream, keys[k].type_id, G_n, keys[k].mask != nullptr));
+    O.key_data[k] = R.keys.back().data;
+    O.key_mask[k] = R.keys.back().mask;
+  }
+  {
+    int j = 0;
+    for (auto& r : reqs) {
+      std::vector<OutColumn> cols;
+      for (size_t a = 0; a < r.aggs.size(); ++a, ++j) {
+        cols.push_back(make_out(alloc, stream, out_types[j], G_n, P.outs[j].nullable));
+        O.out_data[j] = cols.back().data;
+        O.out_mask[j] = cols.back().mask;
+      }
+      R.results.push_back(cols);
+    }
+  }
+  O.counters = counters;
+  if (G_n > 0) {
+    int64_t nslots = (int64_t)cap + 1;
+    int grid = (int)std::min<int64_t>((nslots + 255) / 256, (int64_t)dev.sms * 8);
+    if (opt.profile) ck(cudaEventRecord(events()[2], stream), "event");
+    k_compact<<<grid, 256, 0, stream>>>(P, T, nslots, P.slot_bytes, G_n, O);
+    if (opt.profile) ck(cudaEventRecord(events()[3], stream), "event");
+    ++st.kernels;
+    ck(cudaGetLastError(), "compact launch");
+  }
+  ck(cudaMemcpyAsync(host, counters, 4 * (4 + P.num_keys + P.num_outs), cudaMemcpyDeviceToHost, stream), "null counts d2h");
+  ck(cudaStreamSynchronize(stream), "compact sync");
+  if (host[1]) throw Error(ERR_CUDA, "internal error: compaction found more groups than were counted");
+  if (opt.profile && G_n > 0) {
+    float ms = 0;
+    ck(cudaEventElapsedTime(&ms, events()[2], events()[3]), "event time");
+    st.compact_ms = ms;
+  }
+  for (int k = 0; k < P.num_keys; ++k) R.keys[k].null_count = host[4 + k];
+  {
+    int j = 0;
+    for (auto& cols : R.results)
+      for (auto& c : cols) c.null_count = host[4 + P.num_keys + j++];
+  }
+  } catch (...) {
+    R.release();
+    throw;
+  }
+  if (stats) *stats = st;
+  return R;
+}
+
+}  // namespace gb

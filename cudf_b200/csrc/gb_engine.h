@@ -1,0 +1,107 @@
+// gb_engine.h -- host side of the groupby engine (C++; no torch types).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "gb_plan.h"
+
+namespace gb {
+
+// Error classes mirroring libcudf's (cpp/include/cudf/utilities/error.hpp:177-228):
+// LOGIC = cudf::logic_error, CUDA = cudf::cuda_error, ALLOC = std::bad_alloc.
+enum ErrCode : int { OK = 0, ERR_LOGIC = 1, ERR_CUDA = 2, ERR_ALLOC = 3, ERR_UNSUPPORTED = 4 };
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+struct Column {
+  int32_t type_id;
+  int64_t size;
+  const void* data;
+  const uint32_t* mask;
+  int64_t offset;
+};
+
+struct AggSpec {
+  int32_t kind;
+  int32_t ddof;
+};
+
+struct Request {
+  Column values;
+  std::vector<AggSpec> aggs;
+};
+
+// Stream-ordered device memory resource (the role of rmm's
+// device_memory_resource in cudf::groupby::aggregate).
+struct Allocator {
+  void* (*allocate)(void* ctx, size_t bytes, void* stream);
+  void (*deallocate)(void* ctx, void* p, size_t bytes, void* stream);
+  void* ctx;
+};
+Allocator default_allocator();
+
+struct OutColumn {
+  int32_t type_id = 0;
+  int64_t size = 0;
+  void* data = nullptr;
+  uint32_t* mask = nullptr;
+  int64_t null_count = 0;
+  size_t data_bytes = 0;
+  size_t mask_bytes = 0;
+};
+
+struct Result {
+  int64_t num_groups = 0;
+  std::vector<OutColumn> keys;
+  std::vector<std::vector<OutColumn>> results;
+  Allocator alloc{};
+  cudaStream_t stream = nullptr;
+  void release();  // frees every buffer through alloc
+};
+
+// Engine tunables (an autotuner picks these per size bucket).
+struct Options {
+  int block = 512;             // threads per CTA of the aggregation kernel
+  int blocks_per_sm = 0;       // 0 = occupancy limited
+  int smem_bytes = 96 * 1024;  // shared-memory table bytes per CTA (0 disables the smem stage)
+  double smem_fill = 0.5;      // fraction of smem slots a CTA may claim
+  int64_t smem_max_groups = -1;  // use the smem stage when est. groups <= this (-1: derived)
+  double load_factor = 0.5;    // global table target load
+  int64_t groups_hint = -1;    // caller's group-count estimate (-1: sample)
+  int force_mode = -1;         // -1 auto, 0 global only, 1 smem stage
+  int profile = 0;             // time kernels with CUDA events
+};
+
+struct Stats {
+  int64_t est_groups = 0;
+  int64_t capacity = 0;
+  int mode = 0;     // 0 global, 1 smem stage
+  int retries = 0;
+  int kernels = 0;  // kernels launched by this call
+  double agg_kernel_ms = 0;
+  double compact_ms = 0;
+};
+
+// Builds the plan (validates like cudf::groupby::aggregate,
+// cpp/src/groupby/groupby.cu:202-219, and cpp/src/groupby/groupby.cu:174-190).
+void build_plan(const std::vector<Column>& keys, int null_policy, const std::vector<Request>& reqs,
+                Plan& P, std::vector<int>& out_types);
+
+// The groupby: keys table + requests -> unique keys and one column per
+// requested aggregation, in request order.
+Result aggregate(const std::vector<Column>& keys, int null_policy, const std::vector<Request>& reqs,
+                 cudaStream_t stream, const Allocator& alloc, const Options& opt, Stats* stats);
+
+// type helpers
+int type_width(int type_id);
+bool valid_agg(int type_id, int kind);
+int target_type(int type_id, int kind);
+
+}  // namespace gb

@@ -1,0 +1,164 @@
+/*
+ * cudf_b200.h -- C ABI of the B200 hash groupby-aggregate engine.
+ *
+ * A drop-in for libcudf's hash groupby path:
+ *   cudf::groupby::groupby(keys, null_policy).aggregate(requests, stream, mr)
+ *   (cpp/include/cudf/groupby.hpp:126-197, cpp/src/groupby/groupby.cu:51-62,202-219)
+ * as bound from Python by pylibcudf.groupby.GroupBy.aggregate
+ *   (python/cudf/cudf/_lib/pylibcudf/groupby.pyx:94-155)
+ * and from Java by TableJni.cpp:3124-3155.
+ *
+ * Conventions (the same as libcudf's column_view, cpp/include/cudf/types.hpp):
+ *  - type ids are cudf::type_id values, aggregation kinds cudf::aggregation::Kind
+ *  - null masks are LSB-first 32-bit words (bit i of word i/32 set = row i valid),
+ *    NULL when the column has no nulls; `offset` shifts both data and mask
+ *  - every pointer in a gb_column / gb_out_column is device memory
+ *  - functions return 0 on success or a GB_ERR_* code; gb_last_error() gives the
+ *    message of the calling thread's last failure.  Nothing throws across the ABI.
+ *  - work is stream-ordered on the given cudaStream_t (passed as void*); the call
+ *    returns when the results are complete.
+ */
+#ifndef CUDF_B200_H
+#define CUDF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GB_API __attribute__((visibility("default")))
+#else
+#define GB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GB_OK 0
+#define GB_ERR_LOGIC 1       /* cudf::logic_error: bad arguments, size mismatch, invalid type/agg */
+#define GB_ERR_CUDA 2        /* cudf::cuda_error */
+#define GB_ERR_ALLOC 3       /* std::bad_alloc / rmm::bad_alloc */
+#define GB_ERR_UNSUPPORTED 4 /* outside this engine's scope (e.g. key rows wider than 127 bits) */
+
+#define GB_NULL_EXCLUDE 0    /* cudf::null_policy::EXCLUDE */
+#define GB_NULL_INCLUDE 1    /* cudf::null_policy::INCLUDE */
+
+/* A non-owning column view (cudf::column_view, cpp/include/cudf/column/column_view.hpp). */
+typedef struct gb_column {
+  int32_t type_id;
+  int64_t size;
+  const void* data;
+  const uint32_t* null_mask;
+  int64_t offset;
+} gb_column;
+
+/* One aggregation: cudf::aggregation::Kind plus its parameter (ddof for VARIANCE/STD,
+ * ignored otherwise).  COUNT with null_policy::INCLUDE is kind COUNT_ALL (5). */
+typedef struct gb_agg {
+  int32_t kind;
+  int32_t param;
+} gb_agg;
+
+/* cudf::groupby::aggregation_request (cpp/include/cudf/groupby.hpp:59-62). */
+typedef struct gb_request {
+  gb_column values;
+  int32_t num_aggs;
+  const gb_agg* aggs;
+} gb_request;
+
+/* An owning output column (cudf::column). */
+typedef struct gb_out_column {
+  int32_t type_id;
+  int64_t size;
+  void* data;
+  uint32_t* null_mask;  /* NULL when the column is not nullable */
+  int64_t null_count;
+} gb_out_column;
+
+/* pair<unique_ptr<table>, vector<aggregation_result>> (cpp/include/cudf/groupby.hpp:189-192):
+ * keys[num_keys] are the unique key rows; results[r][j] is aggregation j of request r. */
+typedef struct gb_result {
+  int64_t num_groups;
+  int32_t num_keys;
+  gb_out_column* keys;
+  int32_t num_requests;
+  const int32_t* num_results;
+  gb_out_column** results;
+  void* impl;
+} gb_result;
+
+/* Stream-ordered device memory resource (the `mr` of cudf::groupby::aggregate).
+ * allocate returns NULL on failure. */
+typedef struct gb_allocator {
+  void* (*allocate)(void* ctx, size_t bytes, void* stream);
+  void (*deallocate)(void* ctx, void* ptr, size_t bytes, void* stream);
+  void* ctx;
+} gb_allocator;
+
+typedef struct gb_handle gb_handle;
+
+/* cudf::groupby::groupby::groupby (cpp/src/groupby/groupby.cu:51-62).  The handle does
+ * not own the key columns (cpp/include/cudf/groupby.hpp:111-113).  keys_are_sorted is
+ * accepted for API parity and does not change the results of the hash path. */
+GB_API int gb_create(const gb_column* keys, int32_t num_keys, int32_t null_policy,
+              int32_t keys_are_sorted, gb_handle** out);
+
+/* cudf::groupby::groupby::aggregate (cpp/src/groupby/groupby.cu:202-219).
+ * mr may be NULL (stream-ordered cudaMallocAsync pool). */
+GB_API int gb_aggregate(gb_handle* handle, const gb_request* requests, int32_t num_requests,
+                 void* stream, const gb_allocator* mr, gb_result** out);
+
+/* Frees a result and every column it owns (through the allocator that made it). */
+GB_API void gb_result_free(gb_result* result);
+
+/* Destroys a handle (cudf::groupby::groupby::~groupby). */
+GB_API void gb_destroy(gb_handle* handle);
+
+/* Message of the calling thread's last error ("" if none). */
+GB_API const char* gb_last_error(void);
+
+/* Result type id of an aggregation (cudf::detail::target_type,
+ * cpp/include/cudf/detail/aggregation/aggregation.hpp:1168-1290); 0 if invalid. */
+GB_API int32_t gb_target_type(int32_t type_id, int32_t kind);
+
+/* 1 when the (type, aggregation) pair is supported by the hash path
+ * (cpp/src/groupby/hash/groupby.cu:633-649), else 0. */
+GB_API int32_t gb_is_valid_aggregation(int32_t type_id, int32_t kind);
+
+/* Engine tuning of a handle (no counterpart in libcudf, whose hash path has no
+ * tunables: cpp/src/groupby/hash/groupby.cu:64-67,570-572).  Fields < 0 keep
+ * the default.  force_mode: -1 auto, 0 global table only, 1 shared-memory stage,
+ * 2 hash-partitioned shared-memory aggregation. */
+typedef struct gb_tuning {
+  int32_t block;            /* threads per CTA of the aggregation kernel */
+  int32_t blocks_per_sm;    /* CTAs per SM (0 = occupancy limit) */
+  int32_t smem_bytes;       /* shared-memory table bytes per CTA */
+  int32_t smem_fill_pct;    /* percent of shared slots a CTA may claim */
+  int64_t smem_max_groups;  /* use the shared-memory stage up to this many groups */
+  int32_t load_factor_pct;  /* global table load factor in percent */
+  int32_t force_mode;
+  int64_t groups_hint;      /* caller's estimate of the number of groups (skips sampling) */
+  int32_t profile;          /* 1: time the aggregation and compaction kernels with CUDA events */
+} gb_tuning;
+
+/* What the last gb_aggregate on a handle did. */
+typedef struct gb_stats {
+  int64_t est_groups;
+  int64_t capacity;
+  int32_t mode;             /* 0 global table, 1 shared-memory stage, 2 partitioned */
+  int32_t retries;          /* table-overflow retries */
+  int32_t kernels;          /* kernels launched */
+  double agg_kernel_ms;     /* device time of the aggregation kernel(s) (profile = 1) */
+  double compact_ms;        /* device time of the compaction kernel (profile = 1) */
+} gb_stats;
+
+GB_API int gb_set_tuning(gb_handle* handle, const gb_tuning* tuning);
+GB_API int gb_get_stats(const gb_handle* handle, gb_stats* out);
+
+/* Library version string. */
+GB_API const char* gb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUDF_B200_H */

@@ -1,0 +1,208 @@
+"""Engine vs CPU oracle on seeded random inputs: every supported value type and
+aggregation, nulls, null_policy INCLUDE/EXCLUDE, multi-column keys, both
+aggregation modes, table-overflow retries and sliced (offset) columns."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from parity import run_both
+
+pytestmark = pytest.mark.gpu
+
+
+def _cb():
+    import cudf_b200 as cb
+    from cudf_b200 import aggregation as agg
+    return cb, agg
+
+
+def _rand(rng, type_id, n, lo=-1000, hi=1000):
+    dt = O.NP_DTYPE[type_id]
+    if type_id in (O.FLOAT32, O.FLOAT64):
+        return (rng.normal(size=n) * 100).astype(dt)
+    if type_id == O.BOOL8:
+        return rng.integers(0, 2, n).astype(np.uint8)
+    info = np.iinfo(dt)
+    return rng.integers(max(lo, info.min), min(hi, info.max), n, endpoint=True).astype(dt)
+
+
+ALL_AGGS = ["sum", "min", "max", "count_valid", "count_all", "mean", "sum_of_squares", "variance",
+            "std", "argmin", "argmax"]
+
+
+def _aggs_for(agg, type_id, names):
+    m = {"sum": agg.sum(), "min": agg.min(), "max": agg.max(), "count_valid": agg.count(),
+         "count_all": agg.count(agg.NullPolicy.INCLUDE) if hasattr(agg, "NullPolicy") else None,
+         "mean": agg.mean(), "sum_of_squares": agg.sum_of_squares(), "variance": agg.variance(),
+         "std": agg.std(), "argmin": agg.argmin(), "argmax": agg.argmax(), "product": agg.product()}
+    from cudf_b200.types import NullPolicy
+    m["count_all"] = agg.count(NullPolicy.INCLUDE)
+    return [m[x] for x in names if O.valid_agg(type_id, int(m[x].kind))]
+
+
+@pytest.mark.parametrize("type_id", [O.INT8, O.INT16, O.INT32, O.INT64, O.UINT8, O.UINT16, O.UINT32,
+                                     O.UINT64, O.FLOAT32, O.FLOAT64, O.BOOL8, O.TIMESTAMP_DAYS,
+                                     O.TIMESTAMP_NANOSECONDS, O.DURATION_DAYS, O.DURATION_SECONDS])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_value_types_all_aggs(type_id, mode):
+    cb, agg = _cb()
+    rng = np.random.default_rng(100 + type_id)
+    n = 200_000
+    key = rng.integers(0, 3000, n).astype(np.int32)
+    vals = _rand(rng, type_id, n)
+    valid = rng.random(n) > 0.15
+    aggs = _aggs_for(agg, type_id, ALL_AGGS)
+    run_both([cb.Column.from_numpy(key)], [(cb.Column.from_numpy(vals, valid, type_id), aggs)],
+             tuning={"force_mode": mode})
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_product_small_values(mode):
+    cb, agg = _cb()
+    rng = np.random.default_rng(3)
+    n = 50_000
+    key = rng.integers(0, 20000, n).astype(np.int64)
+    v = rng.integers(-3, 4, n).astype(np.int64)
+    f = rng.uniform(0.5, 1.5, n)
+    run_both([cb.Column.from_numpy(key)],
+             [(cb.Column.from_numpy(v, rng.random(n) > 0.1), [agg.product()]),
+              (cb.Column.from_numpy(f), [agg.product()])], tuning={"force_mode": mode})
+
+
+@pytest.mark.parametrize("policy", [False, True])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_multi_column_nullable_keys(policy, mode):
+    cb, agg = _cb()
+    rng = np.random.default_rng(11)
+    n = 300_000
+    k1 = rng.integers(0, 300, n).astype(np.int32)
+    k2 = rng.integers(0, 40, n).astype(np.int64)
+    kv1, kv2 = rng.random(n) > 0.05, rng.random(n) > 0.05
+    v = rng.integers(0, 10**6, n).astype(np.int64)
+    f = rng.random(n)
+    run_both([cb.Column.from_numpy(k1, kv1), cb.Column.from_numpy(k2, kv2)],
+             [(cb.Column.from_numpy(v), [agg.sum(), agg.count(), agg.max()]),
+              (cb.Column.from_numpy(f, rng.random(n) > 0.3), [agg.sum(), agg.mean(), agg.min()])],
+             include_null_keys=policy, tuning={"force_mode": mode})
+
+
+@pytest.mark.parametrize("ktype", [O.INT8, O.INT16, O.UINT32, O.FLOAT32, O.FLOAT64, O.BOOL8, O.UINT64])
+def test_key_types(ktype):
+    cb, agg = _cb()
+    rng = np.random.default_rng(ktype)
+    n = 100_000
+    if ktype in (O.FLOAT32, O.FLOAT64):
+        base = rng.integers(-50, 50, n).astype(O.NP_DTYPE[ktype]) / 4
+        base[rng.random(n) < 0.02] = np.nan
+        base[rng.random(n) < 0.02] = -0.0
+        k = base
+    else:
+        k = _rand(rng, ktype, n, 0, 200)
+    v = rng.integers(0, 100, n).astype(np.int32)
+    run_both([cb.Column.from_numpy(k, None, ktype)], [(cb.Column.from_numpy(v), [agg.sum(), agg.count()])])
+
+
+def test_three_keys_two_words():
+    cb, agg = _cb()
+    rng = np.random.default_rng(5)
+    n = 200_000
+    ks = [rng.integers(0, 7, n).astype(np.int64), rng.integers(0, 9, n).astype(np.int32),
+          rng.integers(0, 5, n).astype(np.int16)]
+    v = rng.normal(size=n)
+    run_both([cb.Column.from_numpy(k) for k in ks], [(cb.Column.from_numpy(v), [agg.sum(), agg.variance(0)])])
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_all_ones_key_uses_special_slot(mode):
+    cb, agg = _cb()
+    n = 10_000
+    k = np.full(n, -1, dtype=np.int64)
+    k[::3] = 5
+    v = np.arange(n, dtype=np.int64)
+    run_both([cb.Column.from_numpy(k)], [(cb.Column.from_numpy(v), [agg.sum(), agg.min(), agg.count()])],
+             tuning={"force_mode": mode})
+
+
+def test_overflow_retry_with_tiny_hint():
+    cb, agg = _cb()
+    rng = np.random.default_rng(9)
+    n = 400_000
+    k = rng.integers(0, 10**12, n).astype(np.int64)
+    v = rng.integers(-5, 5, n).astype(np.int64)
+    gb, *_ = run_both([cb.Column.from_numpy(k)], [(cb.Column.from_numpy(v), [agg.sum(), agg.count()])],
+                      tuning={"groups_hint": 10, "force_mode": 0})
+    assert gb.stats()["retries"] >= 1
+
+
+def test_sliced_columns_with_offset():
+    cb, agg = _cb()
+    rng = np.random.default_rng(21)
+    n = 100_003
+    k = rng.integers(0, 500, n).astype(np.int32)
+    v = rng.integers(0, 100, n).astype(np.int64)
+    vv = rng.random(n) > 0.2
+    kc = cb.Column.from_numpy(k)
+    vc = cb.Column.from_numpy(v, vv)
+    off, m = 37, 90_001
+    kcs = cb.Column(kc.type_id, kc.data, kc.mask, size=m, offset=off)
+    vcs = cb.Column(vc.type_id, vc.data, vc.mask, size=m, offset=off)
+    run_both([kcs], [(vcs, [agg.sum(), agg.count(), agg.mean(), agg.argmax()])])
+
+
+def test_nan_values_min_max_terminate():
+    cb, agg = _cb()
+    k = np.array([1, 1, 2, 2, 2, 3], dtype=np.int32)
+    v = np.array([np.nan, np.nan, 1.0, np.nan, -2.0, np.inf])
+    run_both([cb.Column.from_numpy(k)], [(cb.Column.from_numpy(v), [agg.min(), agg.max(), agg.argmin(), agg.argmax()])])
+
+
+def test_mismatched_sizes_raise_logic_error():
+    cb, agg = _cb()
+    gb = cb.GroupBy(cb.Table([cb.Column.from_numpy(np.arange(3, dtype=np.int32))]))
+    with pytest.raises(ValueError, match="Size mismatch"):
+        gb.aggregate([cb.GroupByRequest(cb.Column.from_numpy(np.arange(5, dtype=np.int32)), [agg.count()])])
+
+
+def test_invalid_type_aggregation_raises():
+    cb, agg = _cb()
+    gb = cb.GroupBy(cb.Table([cb.Column.from_numpy(np.arange(3, dtype=np.int32))]))
+    ts = cb.Column.from_numpy(np.arange(3, dtype=np.int64), None, O.TIMESTAMP_SECONDS)
+    with pytest.raises(ValueError, match="Invalid type/aggregation"):
+        gb.aggregate([cb.GroupByRequest(ts, [agg.sum()])])
+
+
+def test_results_same_on_a_non_default_stream():
+    """cpp/tests/streams/groupby_test.cpp:25-67: all work on the given stream."""
+    cb, agg = _cb()
+    rng = np.random.default_rng(2)
+    n = 100_000
+    k = cb.Column.from_numpy(rng.integers(0, 100, n).astype(np.int32))
+    v = cb.Column.from_numpy(rng.integers(0, 100, n).astype(np.int64))
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        gb = cb.GroupBy(cb.Table([k]))
+        uk, res = gb.aggregate([cb.GroupByRequest(v, [agg.sum()])], stream=s)
+    s.synchronize()
+    total = int(res[0].columns[0].values().sum().item())
+    assert total == int(v.values().sum().item())
+
+
+@pytest.mark.parametrize("n,card,nulls", [(1_000_000, 1000, 0.0), (2_000_000, 1_000_000, 0.1)])
+def test_config_shapes_medium(n, card, nulls):
+    """The 1M-row pandas configuration and a 2M-row slice of the 100M-row one."""
+    cb, agg = _cb()
+    rng = np.random.default_rng(0)
+    if card == 1000:
+        key = rng.integers(0, 1000, n).astype(np.int32)
+    else:
+        distinct = np.unique(rng.integers(-2**63, 2**63 - 1, card, dtype=np.int64))
+        key = distinct[rng.integers(0, distinct.size, n)]
+    v1 = rng.integers(-10**9, 10**9, n).astype(np.int64)
+    v2 = rng.normal(size=n)
+    v3 = rng.lognormal(size=n).astype(np.float32)
+    masks = [rng.random(n) >= nulls if nulls else None for _ in range(3)]
+    aggs = [agg.sum(), agg.count(), agg.min(), agg.max(), agg.mean()]
+    run_both([cb.Column.from_numpy(key)],
+             [(cb.Column.from_numpy(v1, masks[0]), aggs), (cb.Column.from_numpy(v2, masks[1]), aggs),
+              (cb.Column.from_numpy(v3, masks[2]), aggs)])
