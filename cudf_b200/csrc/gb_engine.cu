@@ -11,6 +11,7 @@
 
 #include "gb_engine.h"
 #include "gb_kernels.cuh"
+#include "gb_partition.cuh"
 
 namespace gb {
 
@@ -279,8 +280,8 @@ void build_plan(const std::vector<Column>& keys, int null_policy, const std::vec
         case K_MAX: add(v, w == 8 ? OP_MAX_U64 : OP_MAX_U32); break;
         case K_SUM_OF_SQUARES: add(v, cat == CAT_F32 ? OP_SQ_F32 : cat == CAT_F64 ? OP_SQ_F64 : OP_SQ_I64); break;
         case K_PRODUCT: add(v, cat == CAT_F32 ? OP_PROD_F32 : cat == CAT_F64 ? OP_PROD_F64 : OP_PROD_I64); break;
-        case K_ARGMIN: add(v, w == 8 ? OP_ARGMIN_R64 : OP_ARGMIN_P32); break;
-        case K_ARGMAX: add(v, w == 8 ? OP_ARGMAX_R64 : OP_ARGMAX_P32); break;
+        case K_ARGMIN: add(v, w == 8 ? OP_ARGMIN_R64 : OP_ARGMIN_P32); P.has_arg = 1; break;
+        case K_ARGMAX: add(v, w == 8 ? OP_ARGMAX_R64 : OP_ARGMAX_P32); P.has_arg = 1; break;
         default: break;
       }
       (void)fl;
@@ -465,8 +466,8 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   R.stream = stream;
   const int64_t n = P.num_rows;
 
-  auto empty_result = [&]() {
-    R.num_groups = 0;
+  // cpp/src/groupby/groupby.cu:216 -- empty input gives empty outputs
+  if (n == 0) {
     for (auto& k : keys) R.keys.push_back(make_out(alloc, stream, k.type_id, 0, k.mask != nullptr));
     int j = 0;
     for (auto& r : reqs) {
@@ -475,12 +476,8 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
         cols.push_back(make_out(alloc, stream, out_types[j], 0, P.outs[j].nullable));
       R.results.push_back(cols);
     }
-    return R;
-  };
-  // cpp/src/groupby/groupby.cu:216 -- empty input gives empty outputs
-  if (n == 0) {
     if (stats) *stats = st;
-    return empty_result();
+    return R;
   }
 
   Scratch S(alloc, stream);
@@ -488,30 +485,39 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   ck(cudaMemsetAsync(counters, 0, 4096, stream), "memset counters");
   uint32_t* host = pinned();
   DevInfo dev = dev_info();
+  SlotTemplate tmpl;
+  build_template(P, tmpl);
 
-  // ---- group-count estimate ----
+  // ---- group-count estimate from a key sample ----
   int64_t est;
+  std::vector<uint32_t> buckets;
+  int64_t nsamp = 0;
   if (opt.groups_hint >= 0) {
     est = std::max<int64_t>(1, opt.groups_hint);
   } else if (n <= 65536) {
     est = n;
   } else {
-    const int64_t nsamp = std::min<int64_t>(n, 1 << 18);
+    nsamp = std::min<int64_t>(n, 1 << 18);
     uint64_t scap = next_pow2((uint64_t)(2 * nsamp));
     size_t sbytes = (scap + 1) * 32;
     uint8_t* ST = (uint8_t*)S.get(sbytes);
+    unsigned int* bk = (unsigned int*)S.get(sizeof(unsigned int) << kBucketBits);
+    ck(cudaMemsetAsync(bk, 0, sizeof(unsigned int) << kBucketBits, stream), "memset buckets");
     SlotTemplate t;
     std::memset(&t, 0, sizeof(t));
     std::memset(&t, 0xFF, 16);
     k_init_slots<<<dev.sms * 4, 256, 0, stream>>>(ST, (int64_t)scap + 1, 32, t);
     TableRef SR{ST, scap - 1, 32, P.key_words, counters + 16};
-    k_sample<<<dev.sms * 4, 256, 0, stream>>>(P, SR, nsamp);
+    k_sample<<<dev.sms * 4, 256, 0, stream>>>(P, SR, nsamp, bk);
     k_sample_stats<<<dev.sms * 4, 256, 0, stream>>>(P, SR);
     st.kernels += 3;
     ck(cudaGetLastError(), "sample launch");
+    buckets.resize((size_t)1 << kBucketBits);
     ck(cudaMemcpyAsync(host, counters + 16, 16 * 4, cudaMemcpyDeviceToHost, stream), "sample d2h");
+    ck(cudaMemcpyAsync(buckets.data(), bk, buckets.size() * 4, cudaMemcpyDeviceToHost, stream), "bucket d2h");
     ck(cudaStreamSynchronize(stream), "sample sync");
     S.put(ST);
+    S.put(bk);
     double d = host[4], f1 = host[5], f2 = host[6], m = host[3];
     if (nsamp >= n) est = (int64_t)d;
     else {
@@ -525,69 +531,217 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   }
   st.est_groups = est;
 
-  // ---- mode and table size ----
-  int scap = 0, sfill = 0;
-  {
-    int sb = std::min(opt.smem_bytes, dev.smem_optin - 1024);
+  // ---- mode ----
+  auto smem_cap_for = [&](int budget) {
+    int sb = std::min(budget, dev.smem_optin - 4096);
+    int c = 0;
     if (sb > 0 && P.slot_bytes <= sb) {
-      scap = 1;
-      while ((int64_t)scap * 2 * P.slot_bytes <= sb) scap *= 2;
-      sfill = std::max(1, (int)(scap * opt.smem_fill));
+      c = 1;
+      while ((int64_t)c * 2 * P.slot_bytes <= sb) c *= 2;
     }
-  }
+    return c;
+  };
+  int scap = smem_cap_for(opt.smem_bytes);
+  int sfill = std::max(1, (int)(scap * opt.smem_fill));
   int64_t smem_max = opt.smem_max_groups >= 0 ? opt.smem_max_groups : 2 * (int64_t)sfill;
-  bool use_smem = scap >= 64 && est <= smem_max;
-  if (opt.force_mode == 0) use_smem = false;
-  if (opt.force_mode == 1 && scap >= 16) use_smem = true;
-  st.mode = use_smem ? 1 : 0;
+  const int scap2 = smem_cap_for(200 * 1024);
+  const int sfill2 = std::max(1, (int)(scap2 * 0.8));
+  const bool part_ok = !P.has_arg && !P.need_second_pass && P.num_vals <= 8 && scap2 >= 256;
+  int nparts = 0;
+  if (part_ok) {
+    double per = scap2 * 0.6;
+    nparts = (int)std::min<uint64_t>(8192, std::max<uint64_t>(2, next_pow2((uint64_t)std::ceil(est / per))));
+  }
+  int mode;
+  if (opt.force_mode >= 0) mode = opt.force_mode;
+  else if (scap >= 64 && est <= smem_max) mode = 1;
+  else if (part_ok && n >= (1 << 20) && est > smem_max) mode = 2;
+  else mode = 0;
+  if (mode == 1 && scap < 16) mode = 0;
+  if (mode == 2 && !part_ok) mode = 0;
+
+  // region sizes of the partitioned path from the sample's bucket counts
+  std::vector<int64_t> pbase, pend;
+  if (mode == 2) {
+    if (buckets.empty()) {  // no sample (hint given or small input): uniform regions
+      buckets.assign((size_t)1 << kBucketBits, 1);
+      nsamp = (int64_t)buckets.size();
+    }
+    int lg = 0;
+    while ((1 << lg) < nparts) ++lg;
+    int per_bucket = kBucketBits - lg;
+    pbase.resize(nparts);
+    pend.resize(nparts);
+    int64_t total = 0, maxload = 0;
+    double samp = 0;
+    for (auto b : buckets) samp += b;
+    for (int p = 0; p < nparts; ++p) {
+      double c = 0;
+      for (int b = p << per_bucket; b < ((p + 1) << per_bucket); ++b) c += buckets[b];
+      int64_t expect = (int64_t)std::ceil((double)n * c / std::max(1.0, samp));
+      int64_t capp = std::max<int64_t>((int64_t)(1.3 * expect), (int64_t)(1.15 * n / nparts)) + 2048;
+      capp = std::min<int64_t>(capp, n);
+      pbase[p] = total;
+      total += (capp + 31) & ~31ll;
+      pend[p] = total;
+      maxload = std::max<int64_t>(maxload, expect);
+    }
+    // heavy skew: one partition would hold far more than its share
+    if (opt.force_mode != 2 && maxload > 4 * (n / nparts) + 4096) mode = (scap >= 64) ? 1 : 0;
+  }
+  st.mode = mode;
 
   uint64_t cap = next_pow2((uint64_t)std::max<double>(1024.0, std::ceil((double)est / opt.load_factor)));
   cap = std::min<uint64_t>(cap, next_pow2((uint64_t)(2 * n + 2)));
   cap = std::max<uint64_t>(cap, 1024);
-  SlotTemplate tmpl;
-  build_template(P, tmpl);
 
   uint8_t* T = nullptr;
   TableRef G{};
-  for (int attempt = 0;; ++attempt) {
-    size_t tbytes = (size_t)(cap + 1) * P.slot_bytes;
-    T = (uint8_t*)S.get(tbytes);
-    k_init_slots<<<dev.sms * 8, 256, 0, stream>>>(T, (int64_t)cap + 1, P.slot_bytes, tmpl);
-    ck(cudaMemsetAsync(counters, 0, 16, stream), "memset counters");
-    G = TableRef{T, cap - 1, P.slot_bytes, P.key_words, counters};
-    int block = opt.block;
+  uint8_t* dense = nullptr;
+  int64_t dense_n = 0;
+  bool done = false;
+
+  if (mode == 2) {
+    // ---- pass 1: scatter rows into hash partitions ----
+    int64_t total = pend.back();
+    int64_t* d_base = (int64_t*)S.get(sizeof(int64_t) * nparts);
+    int64_t* d_end = (int64_t*)S.get(sizeof(int64_t) * nparts);
+    unsigned long long* d_cur = (unsigned long long*)S.get(sizeof(unsigned long long) * nparts);
+    ck(cudaMemcpyAsync(d_base, pbase.data(), 8 * nparts, cudaMemcpyHostToDevice, stream), "h2d");
+    ck(cudaMemcpyAsync(d_end, pend.data(), 8 * nparts, cudaMemcpyHostToDevice, stream), "h2d");
+    ck(cudaMemcpyAsync(d_cur, pbase.data(), 8 * nparts, cudaMemcpyHostToDevice, stream), "h2d");
+    PartArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.nparts = nparts;
+    int lg = 0;
+    while ((1 << lg) < nparts) ++lg;
+    A.shift = 64 - lg;
+    A.base = d_base;
+    A.end = d_end;
+    A.cursor = d_cur;
+    A.keys = (uint64_t*)S.get((size_t)total * 8 * P.key_words);
+    bool any_null = false;
+    for (int v = 0; v < P.num_vals; ++v) {
+      A.vals[v] = S.get((size_t)total * P.vals[v].width);
+      any_null |= P.vals[v].mask != nullptr;
+    }
+    A.bits = any_null ? (uint8_t*)S.get((size_t)total) : nullptr;
+    A.counters = counters;
+    size_t psmem = (size_t)nparts * 12;
     if (opt.profile) ck(cudaEventRecord(events()[0], stream), "event");
-    if (use_smem) {
-      size_t sm = (size_t)scap * P.slot_bytes;
-      ck(cudaFuncSetAttribute(k_aggregate<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), "smem attr");
-      int grid = grid_for((const void*)k_aggregate<true>, block, sm, opt.blocks_per_sm);
-      grid = (int)std::min<int64_t>(grid, (n + block - 1) / block);
-      k_aggregate<true><<<grid, block, sm, stream>>>(P, G, scap, sfill, tmpl);
+    if (P.key_words == 1) {
+      ck(cudaFuncSetAttribute(k_part_scatter<8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem), "attr");
+      int grid = grid_for((const void*)k_part_scatter<8, 1>, 512, psmem, 0);
+      k_part_scatter<8, 1><<<grid, 512, psmem, stream>>>(P, A);
     } else {
-      int grid = grid_for((const void*)k_aggregate<false>, block, 0, opt.blocks_per_sm);
-      grid = (int)std::min<int64_t>(grid, (n + block - 1) / block);
-      k_aggregate<false><<<grid, block, 0, stream>>>(P, G, 1, 0, tmpl);
+      ck(cudaFuncSetAttribute(k_part_scatter<8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem), "attr");
+      int grid = grid_for((const void*)k_part_scatter<8, 2>, 512, psmem, 0);
+      k_part_scatter<8, 2><<<grid, 512, psmem, stream>>>(P, A);
     }
-    if (opt.profile) ck(cudaEventRecord(events()[1], stream), "event");
-    k_finish_count<<<1, 1, 0, stream>>>(P, G);
-    st.kernels += 3;
-    ck(cudaGetLastError(), "aggregate launch");
-    ck(cudaMemcpyAsync(host, counters, 8, cudaMemcpyDeviceToHost, stream), "count d2h");
-    ck(cudaStreamSynchronize(stream), "aggregate sync");
-    if (opt.profile) {
-      float ms = 0;
-      ck(cudaEventElapsedTime(&ms, events()[0], events()[1]), "event time");
-      st.agg_kernel_ms += ms;
+    ++st.kernels;
+    ck(cudaGetLastError(), "partition launch");
+
+    // ---- pass 2: per-partition shared-memory aggregation ----
+    Plan P2 = P;
+    P2.packed_keys = A.keys;
+    for (int v = 0; v < P.num_vals; ++v) {
+      P2.vals[v].data = A.vals[v];
+      P2.vals[v].mask = nullptr;
+      P2.vals[v].offset = 0;
+      P2.vals[v].bits = A.bits;
+      P2.vals[v].bit = v;
     }
-    if (host[1] == 0) break;
-    // table overflow: the kernel stopped inserting; redo with a larger table
-    if (attempt >= 6) throw Error(ERR_CUDA, "hash table overflow");
-    S.put(T);
-    cap *= 4;
-    ++st.retries;
+    uint64_t spill_cap = 1 << 16;
+    int64_t dcap = (int64_t)(est * 1.5) + (int64_t)nparts * 256 + 4096;
+    for (int attempt = 0;; ++attempt) {
+      T = (uint8_t*)S.get((size_t)(spill_cap + 1) * P.slot_bytes);
+      dense = (uint8_t*)S.get((size_t)dcap * P.slot_bytes);
+      k_init_slots<<<dev.sms * 4, 256, 0, stream>>>(T, (int64_t)spill_cap + 1, P.slot_bytes, tmpl);
+      ck(cudaMemsetAsync(counters, 0, 16, stream), "memset");
+      ck(cudaMemsetAsync(counters + 6, 0, 6 * 4, stream), "memset");  // [6] dense overflow, [8] work, [10..11] dense count
+      G = TableRef{T, spill_cap - 1, P.slot_bytes, P.key_words, counters};
+      DenseRef D{dense, dcap, (unsigned long long*)(counters + 10), counters + 6};
+      size_t sm2 = (size_t)scap2 * P.slot_bytes;
+      ck(cudaFuncSetAttribute(k_part_aggregate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2), "attr");
+      int grid = grid_for((const void*)k_part_aggregate, 512, sm2, 0);
+      grid = std::min(grid, nparts);
+      k_part_aggregate<<<grid, 512, sm2, stream>>>(P2, A, G, D, scap2, sfill2, tmpl);
+      if (opt.profile) ck(cudaEventRecord(events()[1], stream), "event");
+      k_finish_count<<<1, 1, 0, stream>>>(P, G);
+      st.kernels += 3;
+      ck(cudaGetLastError(), "partition aggregate launch");
+      ck(cudaMemcpyAsync(host, counters, 48, cudaMemcpyDeviceToHost, stream), "d2h");
+      ck(cudaStreamSynchronize(stream), "partition sync");
+      if (opt.profile && attempt == 0) {
+        float ms = 0;
+        ck(cudaEventElapsedTime(&ms, events()[0], events()[1]), "event time");
+        st.agg_kernel_ms += ms;
+      }
+      if (host[5]) break;  // a region overflowed: fall back to the global table
+      if (host[1] == 0 && host[6] == 0) {
+        done = true;
+        dense_n = (int64_t)(host[10] | ((uint64_t)host[11] << 32));
+        cap = spill_cap;
+        break;
+      }
+      if (attempt >= 6) throw Error(ERR_CUDA, "hash table overflow");
+      if (host[1]) spill_cap *= 8;
+      if (host[6]) dcap *= 2;
+      S.put(T);
+      S.put(dense);
+      ++st.retries;
+    }
+    if (!done) {
+      mode = 0;
+      st.mode = 0;
+      ++st.retries;
+      S.put(T);
+      S.put(dense);
+      dense = nullptr;
+    }
+  }
+
+  if (!done) {
+    for (int attempt = 0;; ++attempt) {
+      size_t tbytes = (size_t)(cap + 1) * P.slot_bytes;
+      T = (uint8_t*)S.get(tbytes);
+      k_init_slots<<<dev.sms * 8, 256, 0, stream>>>(T, (int64_t)cap + 1, P.slot_bytes, tmpl);
+      ck(cudaMemsetAsync(counters, 0, 16, stream), "memset counters");
+      G = TableRef{T, cap - 1, P.slot_bytes, P.key_words, counters};
+      int block = opt.block;
+      if (opt.profile) ck(cudaEventRecord(events()[0], stream), "event");
+      if (mode == 1) {
+        size_t sm = (size_t)scap * P.slot_bytes;
+        ck(cudaFuncSetAttribute(k_aggregate<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), "smem attr");
+        int grid = grid_for((const void*)k_aggregate<true>, block, sm, opt.blocks_per_sm);
+        grid = (int)std::min<int64_t>(grid, (n + block - 1) / block);
+        k_aggregate<true><<<grid, block, sm, stream>>>(P, G, scap, sfill, tmpl);
+      } else {
+        int grid = grid_for((const void*)k_aggregate<false>, block, 0, opt.blocks_per_sm);
+        grid = (int)std::min<int64_t>(grid, (n + block - 1) / block);
+        k_aggregate<false><<<grid, block, 0, stream>>>(P, G, 1, 0, tmpl);
+      }
+      if (opt.profile) ck(cudaEventRecord(events()[1], stream), "event");
+      k_finish_count<<<1, 1, 0, stream>>>(P, G);
+      st.kernels += 3;
+      ck(cudaGetLastError(), "aggregate launch");
+      ck(cudaMemcpyAsync(host, counters, 8, cudaMemcpyDeviceToHost, stream), "count d2h");
+      ck(cudaStreamSynchronize(stream), "aggregate sync");
+      if (opt.profile) {
+        float ms = 0;
+        ck(cudaEventElapsedTime(&ms, events()[0], events()[1]), "event time");
+        st.agg_kernel_ms += ms;
+      }
+      if (host[1] == 0) break;
+      // table overflow: the kernel stopped inserting; redo with a larger table
+      if (attempt >= 6) throw Error(ERR_CUDA, "hash table overflow");
+      S.put(T);
+      cap *= 4;
+      ++st.retries;
+    }
   }
   st.capacity = (int64_t)cap;
-  const int64_t G_n = host[0];
+  const int64_t G_n = (int64_t)host[0] + dense_n;
   R.num_groups = G_n;
 
   if (P.need_second_pass) {
@@ -599,49 +753,54 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
 
   // ---- outputs ----
   try {
-  OutPtrs O;
-  std::memset(&O, 0, sizeof(O));
-  for (int k = 0; k < P.num_keys; ++k) {
-    R.keys.push_back(make_out(alloc, stream, keys[k].type_id, G_n, keys[k].mask != nullptr));
-    O.key_data[k] = R.keys.back().data;
-    O.key_mask[k] = R.keys.back().mask;
-  }
-  {
-    int j = 0;
-    for (auto& r : reqs) {
-      std::vector<OutColumn> cols;
-      for (size_t a = 0; a < r.aggs.size(); ++a, ++j) {
-        cols.push_back(make_out(alloc, stream, out_types[j], G_n, P.outs[j].nullable));
-        O.out_data[j] = cols.back().data;
-        O.out_mask[j] = cols.back().mask;
-      }
-      R.results.push_back(cols);
+    OutPtrs O;
+    std::memset(&O, 0, sizeof(O));
+    for (int k = 0; k < P.num_keys; ++k) {
+      R.keys.push_back(make_out(alloc, stream, keys[k].type_id, G_n, keys[k].mask != nullptr));
+      O.key_data[k] = R.keys.back().data;
+      O.key_mask[k] = R.keys.back().mask;
     }
-  }
-  O.counters = counters;
-  if (G_n > 0) {
-    int64_t nslots = (int64_t)cap + 1;
-    int grid = (int)std::min<int64_t>((nslots + 255) / 256, (int64_t)dev.sms * 8);
+    {
+      int j = 0;
+      for (auto& r : reqs) {
+        std::vector<OutColumn> cols;
+        for (size_t a = 0; a < r.aggs.size(); ++a, ++j) {
+          cols.push_back(make_out(alloc, stream, out_types[j], G_n, P.outs[j].nullable));
+          O.out_data[j] = cols.back().data;
+          O.out_mask[j] = cols.back().mask;
+        }
+        R.results.push_back(cols);
+      }
+    }
+    O.counters = counters;
+    ck(cudaMemsetAsync(counters, 0, 512, stream), "memset");  // position + null counters
     if (opt.profile) ck(cudaEventRecord(events()[2], stream), "event");
-    k_compact<<<grid, 256, 0, stream>>>(P, T, nslots, P.slot_bytes, G_n, O);
+    if (dense_n > 0) {
+      int grid = (int)std::min<int64_t>((dense_n + 255) / 256, (int64_t)dev.sms * 8);
+      k_compact<<<grid, 256, 0, stream>>>(P, dense, dense_n, P.slot_bytes, G_n, 1, O);
+      ++st.kernels;
+    }
+    if (G_n > dense_n) {
+      int64_t nslots = (int64_t)cap + 1;
+      int grid = (int)std::min<int64_t>((nslots + 255) / 256, (int64_t)dev.sms * 8);
+      k_compact<<<grid, 256, 0, stream>>>(P, T, nslots, P.slot_bytes, G_n, 0, O);
+      ++st.kernels;
+    }
     if (opt.profile) ck(cudaEventRecord(events()[3], stream), "event");
-    ++st.kernels;
     ck(cudaGetLastError(), "compact launch");
-  }
-  ck(cudaMemcpyAsync(host, counters, 4 * (4 + P.num_keys + P.num_outs), cudaMemcpyDeviceToHost, stream), "null counts d2h");
-  ck(cudaStreamSynchronize(stream), "compact sync");
-  if (host[1]) throw Error(ERR_CUDA, "internal error: compaction found more groups than were counted");
-  if (opt.profile && G_n > 0) {
-    float ms = 0;
-    ck(cudaEventElapsedTime(&ms, events()[2], events()[3]), "event time");
-    st.compact_ms = ms;
-  }
-  for (int k = 0; k < P.num_keys; ++k) R.keys[k].null_count = host[4 + k];
-  {
+    ck(cudaMemcpyAsync(host, counters, 4 * (4 + P.num_keys + P.num_outs), cudaMemcpyDeviceToHost, stream),
+       "null counts d2h");
+    ck(cudaStreamSynchronize(stream), "compact sync");
+    if (host[1]) throw Error(ERR_CUDA, "internal error: compaction found more groups than were counted");
+    if (opt.profile) {
+      float ms = 0;
+      ck(cudaEventElapsedTime(&ms, events()[2], events()[3]), "event time");
+      st.compact_ms = ms;
+    }
+    for (int k = 0; k < P.num_keys; ++k) R.keys[k].null_count = host[4 + k];
     int j = 0;
     for (auto& cols : R.results)
       for (auto& c : cols) c.null_count = host[4 + P.num_keys + j++];
-  }
   } catch (...) {
     R.release();
     throw;

@@ -57,7 +57,8 @@ __device__ __forceinline__ void update_slot(const Plan& P, uint8_t* slot, int64_
   for (int v = 0; v < P.num_vals; ++v) {
     const ValCol& c = P.vals[v];
     int64_t r = row + c.offset;
-    if (!bit_valid(c.mask, r)) {
+    bool valid = c.bits ? ((c.bits[r] >> c.bit) & 1) : bit_valid(c.mask, r);
+    if (!valid) {
       if (c.nulls_off >= 0) atomicAdd((unsigned int*)(slot + c.nulls_off), 1u);
       continue;
     }
@@ -92,6 +93,13 @@ __device__ __forceinline__ void merge_slot(const Plan& P, const TableRef& G, con
   }
   uint8_t* d = G.T + gi * (int64_t)G.stride;
   atomicAdd((unsigned int*)(d + P.rows_off), *(const uint32_t*)(s + P.rows_off));
+#pragma unroll 1
+  for (int v = 0; v < P.num_vals; ++v) {
+    int off = P.vals[v].nulls_off;
+    if (off < 0) continue;
+    uint32_t nn = *(const uint32_t*)(s + off);
+    if (nn) atomicAdd((unsigned int*)(d + off), nn);
+  }
 #pragma unroll 1
   for (int a = 0; a < P.num_accs; ++a) merge_acc(P, P.accs[a], d, s);
 }
@@ -308,7 +316,7 @@ __device__ __forceinline__ uint64_t finalize(const Plan& P, const OutSpec& o, co
 }
 
 __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ Plan P, const uint8_t* T,
-                                                 int64_t nslots, int stride, int64_t limit,
+                                                 int64_t nslots, int stride, int64_t limit, int dense,
                                                  const __grid_constant__ OutPtrs O)
 {
   using Scan = cub::BlockScan<int, 256>;
@@ -318,7 +326,7 @@ __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ Plan P,
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < nslots; base += step) {
     int64_t i = base + threadIdx.x;
     const uint8_t* slot = T + i * (int64_t)stride;
-    bool occ = i < nslots && slot_occupied(P, slot, i == nslots - 1);
+    bool occ = i < nslots && (dense || slot_occupied(P, slot, i == nslots - 1));
     int local, total;
     Scan(tmp).ExclusiveSum(occ ? 1 : 0, local, total);
     if (threadIdx.x == 0) s_base = total ? atomicAdd(O.counters + 2, (unsigned)total) : 0;
@@ -364,7 +372,11 @@ __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ Plan P,
 
 // ---- group-count estimate from a key sample ----
 // Sample slots: key words (16 B) + u32 count at byte 16; stride 32.
-__global__ void __launch_bounds__(256) k_sample(const __grid_constant__ Plan P, TableRef S, int64_t nsamp)
+// Also counts sampled keys per hash bucket (top kBucketBits bits of the hash)
+// so the partitioned path can size its regions.
+constexpr int kBucketBits = 14;
+__global__ void __launch_bounds__(256) k_sample(const __grid_constant__ Plan P, TableRef S, int64_t nsamp,
+                                                unsigned int* buckets)
 {
   const int64_t n = P.num_rows;
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nsamp;
@@ -373,6 +385,7 @@ __global__ void __launch_bounds__(256) k_sample(const __grid_constant__ Plan P, 
     uint64_t w0, w1;
     if (!pack_key(P, row, w0, w1)) continue;
     uint64_t h = hash_key(w0, w1, P.key_words);
+    atomicAdd(buckets + (h >> (64 - kBucketBits)), 1u);
     bool ins;
     int64_t gi = P.key_words == 1 ? find_or_insert1(S.T, S.stride, S.cap_mask, w0, h, (int)(S.cap_mask + 1), ins)
                                   : find_or_insert2(S.T, S.stride, S.cap_mask, w0, w1, h, (int)(S.cap_mask + 1), ins);

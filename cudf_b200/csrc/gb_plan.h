@@ -83,6 +83,8 @@ struct ValCol {
   int16_t acc_begin;      // accumulators [acc_begin, acc_end) of the first pass
   int16_t acc_end;
   int32_t ddof;           // VARIANCE/STD ddof (one per column; requests with another ddof get a copy)
+  const uint8_t* bits;    // partitioned rows: validity byte per row (bit `bit`), else null
+  int32_t bit;
 };
 
 struct Acc {
@@ -113,7 +115,9 @@ struct Plan {
   int32_t slot_bytes;     // stride of one slot (multiple of 16)
   int32_t rows_off;       // u32 rows-in-group counter
   int32_t need_second_pass;
+  int32_t has_arg;        // ARGMIN/ARGMAX present (needs original row indices)
   int64_t num_rows;
+  const uint64_t* packed_keys;  // partitioned rows: key words per row (key_words each), else null
   KeyCol keys[kMaxKeyCols];
   ValCol vals[kMaxValCols];
   Acc accs[kMaxAccs];

@@ -206,3 +206,59 @@ def test_config_shapes_medium(n, card, nulls):
     run_both([cb.Column.from_numpy(key)],
              [(cb.Column.from_numpy(v1, masks[0]), aggs), (cb.Column.from_numpy(v2, masks[1]), aggs),
               (cb.Column.from_numpy(v3, masks[2]), aggs)])
+
+
+@pytest.mark.parametrize("nulls", [False, True])
+@pytest.mark.parametrize("two_word", [False, True])
+def test_partitioned_mode(nulls, two_word):
+    cb, agg = _cb()
+    rng = np.random.default_rng(31)
+    n = 3_000_000
+    card = 200_000
+    distinct = np.unique(rng.integers(-2**63, 2**63 - 1, card, dtype=np.int64))
+    key = distinct[rng.integers(0, distinct.size, n)]
+    v1 = rng.integers(-10**9, 10**9, n).astype(np.int64)
+    v2 = rng.normal(size=n)
+    v3 = rng.lognormal(size=n).astype(np.float32)
+    ms = [rng.random(n) > 0.1 if nulls else None for _ in range(3)]
+    keys = [cb.Column.from_numpy(key)]
+    if two_word:
+        keys.append(cb.Column.from_numpy(rng.integers(0, 3, n).astype(np.int16), rng.random(n) > 0.05))
+    aggs = [agg.sum(), agg.count(), agg.min(), agg.max(), agg.mean()]
+    gb, *_ = run_both(keys, [(cb.Column.from_numpy(v1, ms[0]), aggs), (cb.Column.from_numpy(v2, ms[1]), aggs),
+                             (cb.Column.from_numpy(v3, ms[2]), aggs + [agg.count(cb.NullPolicy.INCLUDE)])],
+                      include_null_keys=two_word, tuning={"force_mode": 2})
+    assert gb.stats()["mode"] == 2
+
+
+def test_partitioned_mode_is_chosen_for_many_groups():
+    cb, agg = _cb()
+    rng = np.random.default_rng(32)
+    n = 4_000_000
+    key = rng.integers(0, 2**40, n).astype(np.int64)
+    v = rng.integers(0, 100, n).astype(np.int64)
+    gb, *_ = run_both([cb.Column.from_numpy(key)], [(cb.Column.from_numpy(v), [agg.sum(), agg.max()])])
+    assert gb.stats()["mode"] == 2
+
+
+def test_partitioned_spill_when_groups_underestimated():
+    cb, agg = _cb()
+    rng = np.random.default_rng(33)
+    n = 1_500_000
+    key = rng.integers(0, 300_000, n).astype(np.int64)
+    key[::97] = -1  # all-ones key words: the special slot
+    v = rng.integers(-5, 5, n).astype(np.int64)
+    f = rng.random(n).astype(np.float32)
+    run_both([cb.Column.from_numpy(key)], [(cb.Column.from_numpy(v), [agg.sum(), agg.count(), agg.min()]),
+                                           (cb.Column.from_numpy(f, rng.random(n) > 0.2), [agg.mean(), agg.max()])],
+             tuning={"force_mode": 2, "groups_hint": 1000})
+
+
+def test_partitioned_skew_falls_back():
+    cb, agg = _cb()
+    rng = np.random.default_rng(34)
+    n = 2_000_000
+    key = (rng.zipf(1.3, n) % 1_000_003).astype(np.int64)
+    v = rng.integers(0, 1000, n).astype(np.int64)
+    run_both([cb.Column.from_numpy(key)], [(cb.Column.from_numpy(v), [agg.sum(), agg.count(), agg.max()])],
+             tuning={"force_mode": 2})
