@@ -221,6 +221,7 @@ def run_engine(args):
         torch.distributed.barrier()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     kernel_ms = []
+    last_stats = {}
     groups = 0
     launches = 0
     with ClockSampler(dev.index) as clk:
@@ -230,6 +231,7 @@ def run_engine(args):
             uk, res = step()
             st = gb.stats()
             kernel_ms.append(st["agg_kernel_ms"])
+            last_stats = st
             launches += st["kernels"]
             groups = uk.num_rows()
         end.record(stream)
@@ -311,6 +313,7 @@ def run_engine(args):
             "e2e": {"value": world * n / (e_ms * 1e-3), "unit": "rows/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
+            "engine": last_stats,
             "clocks": clk.summary(),
         }
         if not args.no_cpu_baseline and world == 1:

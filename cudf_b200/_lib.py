@@ -51,7 +51,8 @@ class GbTuning(ctypes.Structure):
 class GbStats(ctypes.Structure):
     _fields_ = [("est_groups", ctypes.c_int64), ("capacity", ctypes.c_int64), ("mode", ctypes.c_int32),
                 ("retries", ctypes.c_int32), ("kernels", ctypes.c_int32),
-                ("agg_kernel_ms", ctypes.c_double), ("compact_ms", ctypes.c_double)]
+                ("agg_kernel_ms", ctypes.c_double), ("compact_ms", ctypes.c_double),
+                ("scatter_ms", ctypes.c_double)]
 
 
 class GroupbyError(RuntimeError):

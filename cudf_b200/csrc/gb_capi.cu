@@ -179,6 +179,7 @@ int gb_get_stats(const gb_handle* h, gb_stats* out)
     out->kernels = h->stats.kernels;
     out->agg_kernel_ms = h->stats.agg_kernel_ms;
     out->compact_ms = h->stats.compact_ms;
+    out->scatter_ms = h->stats.scatter_ms;
   });
 }
 

@@ -3,7 +3,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -413,7 +416,7 @@ static void build_template(const Plan& P, SlotTemplate& t)
 // ---------------------------------------------------------------------------
 namespace {
 thread_local uint32_t* t_pinned = nullptr;
-thread_local cudaEvent_t t_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+thread_local cudaEvent_t t_ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 cudaEvent_t* events()
 {
   if (!t_ev[0])
@@ -465,6 +468,13 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   R.alloc = alloc;
   R.stream = stream;
   const int64_t n = P.num_rows;
+  static const bool trace = std::getenv("GB_TRACE") != nullptr;
+  auto t0 = std::chrono::steady_clock::now();
+  auto mark = [&](const char* what) {
+    if (!trace) return;
+    auto t = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "[gb] %-28s %9.3f ms\n", what, std::chrono::duration<double, std::milli>(t - t0).count());
+  };
 
   // cpp/src/groupby/groupby.cu:216 -- empty input gives empty outputs
   if (n == 0) {
@@ -530,6 +540,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     est = std::max<int64_t>(est, 1);
   }
   st.est_groups = est;
+  mark("estimate");
 
   // ---- mode ----
   auto smem_cap_for = [&](int budget) {
@@ -546,11 +557,15 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   int64_t smem_max = opt.smem_max_groups >= 0 ? opt.smem_max_groups : 2 * (int64_t)sfill;
   const int scap2 = smem_cap_for(200 * 1024);
   const int sfill2 = std::max(1, (int)(scap2 * 0.8));
-  const bool part_ok = !P.has_arg && !P.need_second_pass && P.num_vals <= 8 && scap2 >= 256;
+  bool part_ok = !P.has_arg && !P.need_second_pass && P.num_vals <= 8 && scap2 >= 256;
+  for (int a = 0; a < P.num_accs; ++a) {
+    uint8_t op = P.accs[a].op;
+    if (op >= OP_PROD_I64 && op <= OP_PROD_F64) part_ok = false;
+  }
   int nparts = 0;
   if (part_ok) {
     double per = scap2 * 0.6;
-    nparts = (int)std::min<uint64_t>(8192, std::max<uint64_t>(2, next_pow2((uint64_t)std::ceil(est / per))));
+    nparts = (int)std::min<uint64_t>(4096, std::max<uint64_t>(2, next_pow2((uint64_t)std::ceil(est / per))));
   }
   int mode;
   if (opt.force_mode >= 0) mode = opt.force_mode;
@@ -627,19 +642,21 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     }
     A.bits = any_null ? (uint8_t*)S.get((size_t)total) : nullptr;
     A.counters = counters;
-    size_t psmem = (size_t)nparts * 12;
+    mark("partition scratch");
     if (opt.profile) ck(cudaEventRecord(events()[0], stream), "event");
-    if (P.key_words == 1) {
-      ck(cudaFuncSetAttribute(k_part_scatter<8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem), "attr");
-      int grid = grid_for((const void*)k_part_scatter<8, 1>, 512, psmem, 0);
-      k_part_scatter<8, 1><<<grid, 512, psmem, stream>>>(P, A);
-    } else {
-      ck(cudaFuncSetAttribute(k_part_scatter<8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem), "attr");
-      int grid = grid_for((const void*)k_part_scatter<8, 2>, 512, psmem, 0);
-      k_part_scatter<8, 2><<<grid, 512, psmem, stream>>>(P, A);
+    {
+      auto launch = [&](auto kern, int kw, int rpt) {
+        size_t psmem = part_scatter_smem(kw, rpt, nparts);
+        ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem), "attr");
+        int grid = grid_for((const void*)kern, kScatterThreads, psmem, 0);
+        kern<<<grid, kScatterThreads, psmem, stream>>>(P, A);
+      };
+      if (P.key_words == 1) launch(k_part_scatter<1, 16>, 1, 16);
+      else launch(k_part_scatter<2, 16>, 2, 16);
     }
     ++st.kernels;
     ck(cudaGetLastError(), "partition launch");
+    if (opt.profile) ck(cudaEventRecord(events()[4], stream), "event");
 
     // ---- pass 2: per-partition shared-memory aggregation ----
     Plan P2 = P;
@@ -662,10 +679,13 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       G = TableRef{T, spill_cap - 1, P.slot_bytes, P.key_words, counters};
       DenseRef D{dense, dcap, (unsigned long long*)(counters + 10), counters + 6};
       size_t sm2 = (size_t)scap2 * P.slot_bytes;
-      ck(cudaFuncSetAttribute(k_part_aggregate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2), "attr");
-      int grid = grid_for((const void*)k_part_aggregate, 512, sm2, 0);
-      grid = std::min(grid, nparts);
-      k_part_aggregate<<<grid, 512, sm2, stream>>>(P2, A, G, D, scap2, sfill2, tmpl);
+      auto launch2 = [&](auto kern) {
+        ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2), "attr");
+        int grid = grid_for((const void*)kern, 512, sm2, 0);
+        grid = std::min(grid, nparts);
+        kern<<<grid, 512, sm2, stream>>>(P2, A, G, D, scap2, sfill2, tmpl);
+      };
+      launch2(k_part_aggregate<4>);
       if (opt.profile) ck(cudaEventRecord(events()[1], stream), "event");
       k_finish_count<<<1, 1, 0, stream>>>(P, G);
       st.kernels += 3;
@@ -673,10 +693,13 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       ck(cudaMemcpyAsync(host, counters, 48, cudaMemcpyDeviceToHost, stream), "d2h");
       ck(cudaStreamSynchronize(stream), "partition sync");
       if (opt.profile && attempt == 0) {
-        float ms = 0;
+        float ms = 0, ms1 = 0;
         ck(cudaEventElapsedTime(&ms, events()[0], events()[1]), "event time");
+        ck(cudaEventElapsedTime(&ms1, events()[0], events()[4]), "event time");
         st.agg_kernel_ms += ms;
+        st.scatter_ms = ms1;
       }
+      mark("partition passes (synced)");
       if (host[5]) break;  // a region overflowed: fall back to the global table
       if (host[1] == 0 && host[6] == 0) {
         done = true;
@@ -741,6 +764,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     }
   }
   st.capacity = (int64_t)cap;
+  mark("aggregate done");
   const int64_t G_n = (int64_t)host[0] + dense_n;
   R.num_groups = G_n;
 
@@ -792,6 +816,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
        "null counts d2h");
     ck(cudaStreamSynchronize(stream), "compact sync");
     if (host[1]) throw Error(ERR_CUDA, "internal error: compaction found more groups than were counted");
+    mark("compaction (synced)");
     if (opt.profile) {
       float ms = 0;
       ck(cudaEventElapsedTime(&ms, events()[2], events()[3]), "event time");

@@ -85,8 +85,9 @@ struct Stats {
   int mode = 0;     // 0 global, 1 smem stage
   int retries = 0;
   int kernels = 0;  // kernels launched by this call
-  double agg_kernel_ms = 0;
+  double agg_kernel_ms = 0;  // aggregation kernels (partitioned mode: both passes)
   double compact_ms = 0;
+  double scatter_ms = 0;     // partitioned mode: pass 1 alone
 };
 
 // Builds the plan (validates like cudf::groupby::aggregate,

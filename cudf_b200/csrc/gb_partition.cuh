@@ -39,85 +39,172 @@ struct DenseRef {
   unsigned int* overflow;
 };
 
-template <int R, int KW>
-__global__ void __launch_bounds__(512, 1) k_part_scatter(const __grid_constant__ Plan P,
-                                                         const __grid_constant__ PartArgs A)
+// Pass 1.  Each CTA takes tiles of RPT*256 rows.  A tile's rows are counting-
+// sorted by partition in shared memory (keys staged there, then each value
+// column in turn), so every (tile, partition) run leaves as one contiguous
+// write of ~tile/nparts rows instead of scattered 8-byte stores.  256 threads
+// and a 4K-row tile keep the footprint at ~64 KB so three CTAs share an SM;
+// each column's RPT loads per thread are issued back to back.
+// Shared memory: stage[tile * 8*KW] | inv u16[tile] | psort u16[tile] |
+//                hist u32[nparts] | scan u32[nparts] | gbase u64[nparts]
+constexpr int kScatterThreads = 256;
+template <int KW, int RPT>
+__global__ void __launch_bounds__(256, 3) k_part_scatter(const __grid_constant__ Plan P,
+                                                      const __grid_constant__ PartArgs A)
 {
-  extern __shared__ __align__(16) uint8_t sh_raw[];
-  unsigned long long* pbase = (unsigned long long*)sh_raw;
-  unsigned int* hist = (unsigned int*)(pbase + A.nparts);
+  constexpr int T = kScatterThreads;
+  constexpr int TILE = RPT * T;
+  extern __shared__ __align__(16) uint8_t sh[];
+  uint8_t* stage = sh;
+  uint16_t* inv = (uint16_t*)(sh + (size_t)TILE * 8 * KW);
+  uint16_t* psort = inv + TILE;
+  unsigned int* hist = (unsigned int*)(psort + TILE);
+  unsigned int* scan = hist + A.nparts;
+  unsigned long long* gbase = (unsigned long long*)(scan + A.nparts + (A.nparts & 1));
+  using Scan = cub::BlockScan<unsigned, T>;
+  __shared__ typename Scan::TempStorage scan_tmp;
+  __shared__ unsigned int s_valid;
   const int64_t n = P.num_rows;
-  const int64_t tile = (int64_t)blockDim.x * R;
   const bool any_bits = A.bits != nullptr;
-  for (int64_t t0 = (int64_t)blockIdx.x * tile; t0 < n; t0 += (int64_t)gridDim.x * tile) {
-    for (int i = threadIdx.x; i < A.nparts; i += blockDim.x) hist[i] = 0;
+  const int per = (A.nparts + T - 1) / T;  // partitions per thread in the scan
+  for (int64_t t0 = (int64_t)blockIdx.x * TILE; t0 < n; t0 += (int64_t)gridDim.x * TILE) {
+    const int cnt = (int)(n - t0 < (int64_t)TILE ? n - t0 : (int64_t)TILE);
+    for (int i = threadIdx.x; i < A.nparts; i += T) hist[i] = 0;
     __syncthreads();
-    uint64_t k0[R], k1[R];
-    int part[R];
-    unsigned rank[R];
+    // A: keys -> stage, partition ids and ranks
+    uint32_t pr[RPT];
+    if (P.num_keys == 1 && !P.keys[0].mask && P.keys[0].width == 8 && P.keys[0].cat != CAT_F64) {
+      // one plain 64-bit key: load all RPT keys first
+      const unsigned long long* kd = (const unsigned long long*)P.keys[0].data + P.keys[0].offset;
+      uint64_t kk[RPT];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      int64_t row = t0 + (int64_t)r * blockDim.x + threadIdx.x;
-      part[r] = -1;
-      rank[r] = 0;
-      k0[r] = 0;
-      k1[r] = 0;
-      if (row < n) {
+      for (int k = 0; k < RPT; ++k) {
+        int i = k * T + threadIdx.x;
+        kk[k] = i < cnt ? __ldg(kd + t0 + i) : 0;
+      }
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        int i = k * T + threadIdx.x;
+        pr[k] = 0xFFFFFFFFu;
+        if (i < cnt) {
+          ((uint64_t*)stage)[i] = kk[k];
+          unsigned p = (unsigned)(hash_key(kk[k], 0, 1) >> A.shift);
+          pr[k] = (p << 16) | atomicAdd(&hist[p], 1u);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        int i = k * T + threadIdx.x;
+        pr[k] = 0xFFFFFFFFu;
         uint64_t w0, w1;
-        if (pack_key(P, row, w0, w1)) {
-          k0[r] = w0;
-          k1[r] = w1;
-          part[r] = (int)(hash_key(w0, w1, KW) >> A.shift);
+        if (i < cnt && pack_key(P, t0 + i, w0, w1)) {
+          if (KW == 1) ((uint64_t*)stage)[i] = w0;
+          else ((ulonglong2*)stage)[i] = make_ulonglong2(w0, w1);
+          unsigned p = (unsigned)(hash_key(w0, w1, KW) >> A.shift);
+          pr[k] = (p << 16) | atomicAdd(&hist[p], 1u);
         }
       }
     }
-#pragma unroll
-    for (int r = 0; r < R; ++r)
-      if (part[r] >= 0) rank[r] = atomicAdd(&hist[part[r]], 1u);
     __syncthreads();
-    for (int i = threadIdx.x; i < A.nparts; i += blockDim.x) {
-      unsigned c = hist[i];
-      pbase[i] = c ? atomicAdd(&A.cursor[i], (unsigned long long)c) : 0ull;
-    }
-    __syncthreads();
-    int64_t pos[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      pos[r] = -1;
-      if (part[r] < 0) continue;
-      int64_t p = (int64_t)(pbase[part[r]] + rank[r]);
-      if (p >= A.end[part[r]]) {
-        atomicOr(A.counters + 5, 1u);
-        continue;
+    // B: reserve each partition's run; exclusive scan of the histogram
+    unsigned mine = 0;
+    for (int q = threadIdx.x * per; q < min(A.nparts, (threadIdx.x + 1) * per); ++q) {
+      unsigned h = hist[q];
+      mine += h;
+      if (h) {
+        unsigned long long g = atomicAdd(&A.cursor[q], (unsigned long long)h);
+        gbase[q] = g;
+        if ((int64_t)(g + h) > A.end[q]) atomicOr(A.counters + 5, 1u);
       }
-      pos[r] = p;
-      if (KW == 1) A.keys[p] = k0[r];
-      else *(ulonglong2*)(A.keys + 2 * p) = make_ulonglong2(k0[r], k1[r]);
     }
-    uint32_t vb[R];
+    unsigned off, total;
+    Scan(scan_tmp).ExclusiveSum(mine, off, total);
+    for (int q = threadIdx.x * per; q < min(A.nparts, (threadIdx.x + 1) * per); ++q) {
+      scan[q] = off;
+      off += hist[q];
+    }
+    if (threadIdx.x == 0) s_valid = total;
+    __syncthreads();
+    // C: sorted order
 #pragma unroll
-    for (int r = 0; r < R; ++r) vb[r] = 0;
+    for (int k = 0; k < RPT; ++k) {
+      if (pr[k] == 0xFFFFFFFFu) continue;
+      unsigned p = pr[k] >> 16;
+      unsigned s = scan[p] + (pr[k] & 0xFFFFu);
+      inv[s] = (uint16_t)(k * T + threadIdx.x);
+      psort[s] = (uint16_t)p;
+    }
+    __syncthreads();
+    const int nvalid = (int)s_valid;
+    // D: keys out
+    for (int s = threadIdx.x; s < nvalid; s += T) {
+      unsigned p = psort[s];
+      int64_t g = (int64_t)gbase[p] + (s - (int)scan[p]);
+      if (g >= A.end[p]) continue;
+      if (KW == 1) A.keys[g] = ((const uint64_t*)stage)[inv[s]];
+      else ((ulonglong2*)A.keys)[g] = ((const ulonglong2*)stage)[inv[s]];
+    }
+    // E: each value column through the stage
+    uint32_t vb[RPT];
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) vb[k] = 0;
 #pragma unroll 1
     for (int v = 0; v < P.num_vals; ++v) {
       const ValCol& c = P.vals[v];
-      uint64_t x[R];
+      uint64_t x[RPT];
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        int64_t row = t0 + (int64_t)r * blockDim.x + threadIdx.x + c.offset;
-        x[r] = pos[r] >= 0 ? load_bits(c.data, row, c.width) : 0;
-        if (any_bits && pos[r] >= 0 && bit_valid(c.mask, row)) vb[r] |= 1u << v;
+      for (int k = 0; k < RPT; ++k) {
+        int i = k * T + threadIdx.x;
+        x[k] = pr[k] != 0xFFFFFFFFu ? load_bits(c.data, t0 + i + c.offset, c.width) : 0;
       }
+      if (any_bits && c.mask) {
 #pragma unroll
-      for (int r = 0; r < R; ++r)
-        if (pos[r] >= 0) store_width(A.vals[v], pos[r], c.width, x[r]);
+        for (int k = 0; k < RPT; ++k)
+          if (pr[k] != 0xFFFFFFFFu && bit_valid(c.mask, t0 + k * T + threadIdx.x + c.offset)) vb[k] |= 1u << v;
+      } else if (any_bits) {
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) vb[k] |= 1u << v;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < RPT; ++k)
+        if (pr[k] != 0xFFFFFFFFu) store_width(stage, k * T + threadIdx.x, c.width, x[k]);
+      __syncthreads();
+      for (int s = threadIdx.x; s < nvalid; s += T) {
+        unsigned p = psort[s];
+        int64_t g = (int64_t)gbase[p] + (s - (int)scan[p]);
+        if (g >= A.end[p]) continue;
+        int i = inv[s];
+        switch (c.width) {
+          case 1: ((uint8_t*)A.vals[v])[g] = stage[i]; break;
+          case 2: ((uint16_t*)A.vals[v])[g] = ((const uint16_t*)stage)[i]; break;
+          case 4: ((uint32_t*)A.vals[v])[g] = ((const uint32_t*)stage)[i]; break;
+          default: ((uint64_t*)A.vals[v])[g] = ((const uint64_t*)stage)[i]; break;
+        }
+      }
     }
     if (any_bits) {
+      __syncthreads();
 #pragma unroll
-      for (int r = 0; r < R; ++r)
-        if (pos[r] >= 0) A.bits[pos[r]] = (uint8_t)vb[r];
+      for (int k = 0; k < RPT; ++k)
+        if (pr[k] != 0xFFFFFFFFu) stage[k * T + threadIdx.x] = (uint8_t)vb[k];
+      __syncthreads();
+      for (int s = threadIdx.x; s < nvalid; s += T) {
+        unsigned p = psort[s];
+        int64_t g = (int64_t)gbase[p] + (s - (int)scan[p]);
+        if (g < A.end[p]) A.bits[g] = stage[inv[s]];
+      }
     }
     __syncthreads();
   }
+}
+
+// shared-memory bytes k_part_scatter<KW, RPT> needs
+inline size_t part_scatter_smem(int kw, int rpt, int nparts)
+{
+  size_t tile = (size_t)rpt * kScatterThreads;
+  return tile * 8 * kw + tile * 4 + (size_t)nparts * 8 + 8 + (size_t)nparts * 8;
 }
 
 // Shared-memory find-or-insert (bounded probes); null when the key does not
@@ -160,8 +247,99 @@ __device__ __forceinline__ uint8_t* smem_slot(uint8_t* smem, int stride, uint64_
   return nullptr;
 }
 
-// P2 is the plan with value columns redirected to the partitioned arrays
-// (offset 0, `bits` validity) and packed_keys set.
+// ---- explicit shared-memory operations (32-bit shared-window addresses) ----
+__device__ __forceinline__ void sred_add_u32(uint32_t a, uint32_t v) { asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory"); }
+__device__ __forceinline__ void sred_add_u64(uint32_t a, uint64_t v) { asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); }
+__device__ __forceinline__ void sred_add_f32(uint32_t a, float v) { asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory"); }
+__device__ __forceinline__ void sred_add_f64(uint32_t a, double v) { asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory"); }
+__device__ __forceinline__ void sred_min_u32(uint32_t a, uint32_t v) { asm volatile("red.shared.min.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory"); }
+__device__ __forceinline__ void sred_max_u32(uint32_t a, uint32_t v) { asm volatile("red.shared.max.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory"); }
+__device__ __forceinline__ void sred_min_u64(uint32_t a, uint64_t v) { asm volatile("red.shared.min.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); }
+__device__ __forceinline__ void sred_max_u64(uint32_t a, uint64_t v) { asm volatile("red.shared.max.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); }
+__device__ __forceinline__ uint32_t sld_u32(uint32_t a)
+{
+  uint32_t v;
+  asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ uint64_t sld_u64(uint32_t a)
+{
+  uint64_t v;
+  asm volatile("ld.volatile.shared.u64 %0, [%1];" : "=l"(v) : "r"(a));
+  return v;
+}
+
+// Ops the partitioned path supports (PRODUCT and ARGMIN/ARGMAX plans use the
+// other modes).
+__device__ __forceinline__ bool part_op_ok(uint8_t op)
+{
+  return op <= OP_MAX_U64 || op == OP_SQ_I64 || op == OP_SQ_F32 || op == OP_SQ_F64;
+}
+
+// Applies one valid value (raw bits) of column c to a shared slot at `sa`.
+__device__ __forceinline__ void sapply(const Plan& P, const ValCol& c, uint32_t sa, uint64_t bits)
+{
+  int64_t iv = 0;
+  float f = 0.f;
+  double d = 0.0;
+  switch (c.cat) {
+    case CAT_SIGNED: iv = sign_extend(bits, c.width); break;
+    case CAT_BOOL: iv = bits != 0; break;
+    case CAT_UNSIGNED: iv = (int64_t)bits; break;
+    case CAT_F32: f = __uint_as_float((uint32_t)bits); d = f; break;
+    default: d = __longlong_as_double((long long)bits); break;
+  }
+#pragma unroll 1
+  for (int a = c.acc_begin; a < c.acc_end; ++a) {
+    const Acc A = P.accs[a];
+    uint32_t p = sa + A.off;
+    switch (A.op) {
+      case OP_SUM_I64: sred_add_u64(p, (uint64_t)iv); break;
+      case OP_SUM_I32: sred_add_u32(p, (uint32_t)iv); break;
+      case OP_SUM_F32: sred_add_f32(p, f); break;
+      case OP_SUM_F64: sred_add_f64(p, d); break;
+      case OP_MIN_U32: case OP_MAX_U32: {
+        bool mn = A.op == OP_MIN_U32;
+        uint32_t v = c.cat == CAT_F32 ? ord32_f(f, mn)
+                     : (c.cat == CAT_UNSIGNED || c.cat == CAT_BOOL) ? (uint32_t)iv
+                                                                    : ((uint32_t)(int32_t)iv ^ 0x80000000u);
+        uint32_t cur = sld_u32(p);
+        if (mn ? v < cur : v > cur) { if (mn) sred_min_u32(p, v); else sred_max_u32(p, v); }
+        break;
+      }
+      case OP_MIN_U64: case OP_MAX_U64: {
+        bool mn = A.op == OP_MIN_U64;
+        uint64_t v = c.cat == CAT_F64 ? ord64_f(d, mn)
+                     : c.cat == CAT_UNSIGNED ? bits : ((uint64_t)iv ^ 0x8000000000000000ull);
+        uint64_t cur = sld_u64(p);
+        if (mn ? v < cur : v > cur) { if (mn) sred_min_u64(p, v); else sred_max_u64(p, v); }
+        break;
+      }
+      case OP_SQ_I64: sred_add_u64(p, (uint64_t)iv * (uint64_t)iv); break;
+      case OP_SQ_F32: sred_add_f32(p, f * f); break;
+      case OP_SQ_F64: sred_add_f64(p, d * d); break;
+      default: break;
+    }
+  }
+}
+
+// A row whose key did not fit the shared table: global table, generic update.
+__device__ __noinline__ void spill_row(const Plan& P2, const TableRef& G, uint64_t w0, uint64_t w1,
+                                       uint64_t h, int64_t r, unsigned int* s_new)
+{
+  int64_t gi = global_slot(P2, G, w0, w1, h, s_new);
+  if (gi < 0) {
+    atomicOr(G.counters + 1, 1u);
+    return;
+  }
+  update_slot(P2, G.T + gi * (int64_t)G.stride, r);
+}
+
+// Pass 2.  P2 is the plan with value columns redirected to the partitioned
+// arrays (offset 0, `bits` validity) and packed_keys set.  R rows per thread
+// per step: keys first, then the shared slot of each, then column by column
+// the values (R loads in flight) and their shared-memory updates.
+template <int R>
 __global__ void __launch_bounds__(512, 1) k_part_aggregate(const __grid_constant__ Plan P2,
                                                            const __grid_constant__ PartArgs A,
                                                            TableRef G, DenseRef D, int scap, int sfill,
@@ -178,6 +356,8 @@ __global__ void __launch_bounds__(512, 1) k_part_aggregate(const __grid_constant
   const int nw = stride / 16;
   const uint64_t smask = (uint64_t)scap - 1;
   const int per = (scap + blockDim.x - 1) / blockDim.x;
+  const bool have_bits = A.bits != nullptr;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
   for (;;) {
     if (threadIdx.x == 0) {
       s_part = (int)atomicAdd(A.counters + 8, 1u);
@@ -193,26 +373,59 @@ __global__ void __launch_bounds__(512, 1) k_part_aggregate(const __grid_constant
     if (p >= A.nparts) break;
     const int64_t b = A.base[p];
     const int64_t e = min((int64_t)A.cursor[p], A.end[p]);
-    for (int64_t r = b + threadIdx.x; r < e; r += blockDim.x) {
-      uint64_t w0, w1 = 0;
-      if (P2.key_words == 1) w0 = P2.packed_keys[r];
-      else {
-        ulonglong2 kk = *(const ulonglong2*)(P2.packed_keys + 2 * r);
-        w0 = kk.x;
-        w1 = kk.y;
+    for (int64_t r0 = b; r0 < e; r0 += (int64_t)R * blockDim.x) {
+      uint64_t k0[R], k1[R];
+      uint32_t vb[R], sa[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        int64_t r = r0 + (int64_t)j * blockDim.x + threadIdx.x;
+        k0[j] = kEmpty;
+        k1[j] = 0;
+        vb[j] = 0xFFFFFFFFu;
+        if (r < e) {
+          if (P2.key_words == 1) k0[j] = P2.packed_keys[r];
+          else {
+            ulonglong2 kk = *(const ulonglong2*)(P2.packed_keys + 2 * r);
+            k0[j] = kk.x;
+            k1[j] = kk.y;
+          }
+          if (have_bits) vb[j] = A.bits[r];
+        }
       }
-      uint64_t h = hash_key(w0, w1, P2.key_words);
-      uint8_t* slot = smem_slot(smem, stride, smask, sfill, &s_used, P2.key_words, w0, w1, h);
-      if (slot == nullptr) {
-        s_spill = 1;
-        int64_t gi = global_slot(P2, G, w0, w1, h, &s_new);
-        if (gi < 0) {
-          atomicOr(G.counters + 1, 1u);
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        int64_t r = r0 + (int64_t)j * blockDim.x + threadIdx.x;
+        sa[j] = 0;
+        if (r >= e) continue;
+        uint64_t h = hash_key(k0[j], k1[j], P2.key_words);
+        uint8_t* slot = smem_slot(smem, stride, smask, sfill, &s_used, P2.key_words, k0[j], k1[j], h);
+        if (slot == nullptr) {
+          s_spill = 1;
+          spill_row(P2, G, k0[j], k1[j], h, r, &s_new);
           continue;
         }
-        slot = G.T + gi * (int64_t)stride;
+        sa[j] = sbase + (uint32_t)(slot - smem);
+        sred_add_u32(sa[j] + P2.rows_off, 1u);
       }
-      update_slot(P2, slot, r);
+#pragma unroll 1
+      for (int v = 0; v < P2.num_vals; ++v) {
+        const ValCol& c = P2.vals[v];
+        uint64_t x[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          int64_t r = r0 + (int64_t)j * blockDim.x + threadIdx.x;
+          x[j] = (sa[j] && ((vb[j] >> v) & 1)) ? load_bits(c.data, r, c.width) : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          if (!sa[j]) continue;
+          if (!((vb[j] >> v) & 1)) {
+            if (c.nulls_off >= 0) sred_add_u32(sa[j] + c.nulls_off, 1u);
+            continue;
+          }
+          sapply(P2, c, sa[j], x[j]);
+        }
+      }
     }
     __syncthreads();
     if (s_spill) {

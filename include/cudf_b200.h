@@ -150,6 +150,7 @@ typedef struct gb_stats {
   int32_t kernels;          /* kernels launched */
   double agg_kernel_ms;     /* device time of the aggregation kernel(s) (profile = 1) */
   double compact_ms;        /* device time of the compaction kernel (profile = 1) */
+  double scatter_ms;        /* partitioned mode: device time of the partition pass (profile = 1) */
 } gb_stats;
 
 GB_API int gb_set_tuning(gb_handle* handle, const gb_tuning* tuning);

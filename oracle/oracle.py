@@ -216,6 +216,8 @@ def sort_order(key_cols) -> np.ndarray:
     arrays = []
     for data, valid in reversed(list(key_cols)):
         d = np.asarray(data)
+        if valid is not None:  # the value under a null is arbitrary: sort nulls as 0
+            d = np.where(np.asarray(valid, dtype=bool), d, np.zeros((), d.dtype))
         if d.dtype.kind == "f":
             nan = np.isnan(d)
             d = np.where(nan, 0, d)
