@@ -338,7 +338,15 @@ void build_plan(const std::vector<Column>& keys, int null_policy, const std::vec
       P.need_second_pass = 1;
     }
   P.num_accs = na;
-  P.slot_bytes = (off + 15) & ~15;
+  // stride: an odd multiple of 8 bytes (16 for two-word keys, whose 128-bit
+  // CAS needs 16-byte alignment) so that one field of 32 different slots
+  // falls into many shared-memory banks
+  {
+    int unit = P.key_words == 2 ? 16 : 8;
+    int q = (off + unit - 1) / unit;
+    if ((q & 1) == 0) ++q;
+    P.slot_bytes = q * unit;
+  }
   if (P.slot_bytes > kMaxSlotBytes) throw Error(ERR_UNSUPPORTED, "too many aggregations in one call");
   // reorder accs by column so each column owns a contiguous range
   std::stable_sort(P.accs, P.accs + na, [](const Acc& a, const Acc& b) { return a.col < b.col; });
@@ -398,7 +406,7 @@ void build_plan(const std::vector<Column>& keys, int null_policy, const std::vec
 static void build_template(const Plan& P, SlotTemplate& t)
 {
   std::memset(&t, 0, sizeof(t));
-  uint8_t* b = (uint8_t*)t.w;
+  uint8_t* b = (uint8_t*)&t.w[0];
   std::memset(b, 0xFF, 8 * P.key_words);
   for (int a = 0; a < P.num_accs; ++a) {
     uint8_t* p = b + P.accs[a].off;
@@ -516,7 +524,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     SlotTemplate t;
     std::memset(&t, 0, sizeof(t));
     std::memset(&t, 0xFF, 16);
-    k_init_slots<<<dev.sms * 4, 256, 0, stream>>>(ST, (int64_t)scap + 1, 32, t);
+    k_init_slots<<<dev.sms * 4, 256, 0, stream>>>(ST, (int64_t)scap + 1, 32, t);  // 16 B key | u32 count
     TableRef SR{ST, scap - 1, 32, P.key_words, counters + 16};
     k_sample<<<dev.sms * 4, 256, 0, stream>>>(P, SR, nsamp, bk);
     k_sample_stats<<<dev.sms * 4, 256, 0, stream>>>(P, SR);
@@ -651,8 +659,14 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
         int grid = grid_for((const void*)kern, kScatterThreads, psmem, 0);
         kern<<<grid, kScatterThreads, psmem, stream>>>(P, A);
       };
-      if (P.key_words == 1) launch(k_part_scatter<1, 16>, 1, 16);
-      else launch(k_part_scatter<2, 16>, 2, 16);
+      int budget = dev.smem_optin - 4096;
+      if (P.key_words == 1) {
+        if ((int)part_scatter_smem(1, 32, nparts) <= budget) launch(k_part_scatter<1, 32>, 1, 32);
+        else launch(k_part_scatter<1, 16>, 1, 16);
+      } else {
+        if ((int)part_scatter_smem(2, 16, nparts) <= budget) launch(k_part_scatter<2, 16>, 2, 16);
+        else launch(k_part_scatter<2, 8>, 2, 8);
+      }
     }
     ++st.kernels;
     ck(cudaGetLastError(), "partition launch");

@@ -17,8 +17,11 @@ namespace gb {
 
 constexpr int kMaxSlotBytes = 1024;
 
+// Identity contents of an empty slot, as 8-byte words (slot strides are
+// multiples of 8; an odd multiple spreads a field of consecutive slots over
+// all shared-memory banks).
 struct SlotTemplate {
-  uint4 w[kMaxSlotBytes / 16];
+  unsigned long long w[kMaxSlotBytes / 8];
 };
 
 struct TableRef {
@@ -31,13 +34,13 @@ struct TableRef {
 
 __global__ void k_init_slots(uint8_t* T, int64_t nslots, int stride, const __grid_constant__ SlotTemplate tmpl)
 {
-  int nw = stride / 16;
+  int nw = stride / 8;
   int64_t total = nslots * nw;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
        i += (int64_t)gridDim.x * blockDim.x) {
     int64_t s = i / nw;
     int w = (int)(i - s * nw);
-    *(uint4*)(T + s * stride + w * 16) = tmpl.w[w];
+    *(unsigned long long*)(T + s * stride + w * 8) = tmpl.w[w];
   }
 }
 
@@ -117,11 +120,11 @@ __global__ void __launch_bounds__(512) k_aggregate(const __grid_constant__ Plan 
   __shared__ unsigned int s_new, s_used;
   if (threadIdx.x == 0) { s_new = 0; s_used = 0; }
   if (USE_SMEM) {
-    int nw = G.stride / 16;
+    int nw = G.stride / 8;
     for (int i = threadIdx.x; i < scap * nw; i += blockDim.x) {
       int s = i / nw;
       int w = i - s * nw;
-      *(uint4*)(smem + s * G.stride + w * 16) = tmpl.w[w];
+      *(unsigned long long*)(smem + s * G.stride + w * 8) = tmpl.w[w];
     }
   }
   __syncthreads();

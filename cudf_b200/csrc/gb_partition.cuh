@@ -39,21 +39,30 @@ struct DenseRef {
   unsigned int* overflow;
 };
 
-// Pass 1.  Each CTA takes tiles of RPT*256 rows.  A tile's rows are counting-
-// sorted by partition in shared memory (keys staged there, then each value
-// column in turn), so every (tile, partition) run leaves as one contiguous
-// write of ~tile/nparts rows instead of scattered 8-byte stores.  256 threads
-// and a 4K-row tile keep the footprint at ~64 KB so three CTAs share an SM;
-// each column's RPT loads per thread are issued back to back.
+// Pass 1.  Each CTA takes tiles of RPT*512 rows.  It first asks L2 for the
+// tile's value columns and masks (prefetch.global.L2, one per 128-byte line),
+// then loads the keys, counting-sorts the tile's rows by partition in shared
+// memory (keys staged there), reserves one run per (tile, partition) with a
+// global atomic, and finally writes every column in partition order: values
+// are gathered from L2 by the sorted row index, and consecutive threads write
+// consecutive positions of a partition's run, so stores leave in runs of
+// ~tile/nparts rows.
 // Shared memory: stage[tile * 8*KW] | inv u16[tile] | psort u16[tile] |
 //                hist u32[nparts] | scan u32[nparts] | gbase u64[nparts]
-constexpr int kScatterThreads = 256;
+constexpr int kScatterThreads = 512;
+
+__device__ __forceinline__ void prefetch_l2(const void* p)
+{
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 template <int KW, int RPT>
-__global__ void __launch_bounds__(256, 3) k_part_scatter(const __grid_constant__ Plan P,
-                                                      const __grid_constant__ PartArgs A)
+__global__ void __launch_bounds__(512, 1) k_part_scatter(const __grid_constant__ Plan P,
+                                                         const __grid_constant__ PartArgs A)
 {
   constexpr int T = kScatterThreads;
   constexpr int TILE = RPT * T;
+  constexpr int U = 8;  // sorted rows per thread per gather batch
   extern __shared__ __align__(16) uint8_t sh[];
   uint8_t* stage = sh;
   uint16_t* inv = (uint16_t*)(sh + (size_t)TILE * 8 * KW);
@@ -69,12 +78,23 @@ __global__ void __launch_bounds__(256, 3) k_part_scatter(const __grid_constant__
   const int per = (A.nparts + T - 1) / T;  // partitions per thread in the scan
   for (int64_t t0 = (int64_t)blockIdx.x * TILE; t0 < n; t0 += (int64_t)gridDim.x * TILE) {
     const int cnt = (int)(n - t0 < (int64_t)TILE ? n - t0 : (int64_t)TILE);
+    // value columns and masks of this tile into L2 while the keys are sorted
+    for (int v = 0; v < P.num_vals; ++v) {
+      const ValCol& c = P.vals[v];
+      const uint8_t* base = (const uint8_t*)c.data + (t0 + c.offset) * c.width;
+      int64_t bytes = (int64_t)cnt * c.width;
+      for (int64_t o = (int64_t)threadIdx.x * 128; o < bytes; o += (int64_t)T * 128) prefetch_l2(base + o);
+      if (c.mask) {
+        int64_t w = (t0 + c.offset) / 32 + (int64_t)threadIdx.x * 32;
+        if (w <= (t0 + c.offset + cnt - 1) / 32) prefetch_l2(c.mask + w);
+      }
+    }
     for (int i = threadIdx.x; i < A.nparts; i += T) hist[i] = 0;
     __syncthreads();
     // A: keys -> stage, partition ids and ranks
     uint32_t pr[RPT];
-    if (P.num_keys == 1 && !P.keys[0].mask && P.keys[0].width == 8 && P.keys[0].cat != CAT_F64) {
-      // one plain 64-bit key: load all RPT keys first
+    if (KW == 1 && P.num_keys == 1 && !P.keys[0].mask && P.keys[0].width == 8 && P.keys[0].cat != CAT_F64) {
+      // one plain 64-bit key: all RPT loads in flight first
       const unsigned long long* kd = (const unsigned long long*)P.keys[0].data + P.keys[0].offset;
       uint64_t kk[RPT];
 #pragma unroll
@@ -137,63 +157,53 @@ __global__ void __launch_bounds__(256, 3) k_part_scatter(const __grid_constant__
     }
     __syncthreads();
     const int nvalid = (int)s_valid;
-    // D: keys out
-    for (int s = threadIdx.x; s < nvalid; s += T) {
-      unsigned p = psort[s];
-      int64_t g = (int64_t)gbase[p] + (s - (int)scan[p]);
-      if (g >= A.end[p]) continue;
-      if (KW == 1) A.keys[g] = ((const uint64_t*)stage)[inv[s]];
-      else ((ulonglong2*)A.keys)[g] = ((const ulonglong2*)stage)[inv[s]];
-    }
-    // E: each value column through the stage
-    uint32_t vb[RPT];
+    // D: every column out in partition order, U sorted rows per thread at a time
+    for (int sb = 0; sb < nvalid; sb += U * T) {
+      int64_t g[U];
+      int ii[U];
 #pragma unroll
-    for (int k = 0; k < RPT; ++k) vb[k] = 0;
-#pragma unroll 1
-    for (int v = 0; v < P.num_vals; ++v) {
-      const ValCol& c = P.vals[v];
-      uint64_t x[RPT];
-#pragma unroll
-      for (int k = 0; k < RPT; ++k) {
-        int i = k * T + threadIdx.x;
-        x[k] = pr[k] != 0xFFFFFFFFu ? load_bits(c.data, t0 + i + c.offset, c.width) : 0;
-      }
-      if (any_bits && c.mask) {
-#pragma unroll
-        for (int k = 0; k < RPT; ++k)
-          if (pr[k] != 0xFFFFFFFFu && bit_valid(c.mask, t0 + k * T + threadIdx.x + c.offset)) vb[k] |= 1u << v;
-      } else if (any_bits) {
-#pragma unroll
-        for (int k = 0; k < RPT; ++k) vb[k] |= 1u << v;
-      }
-      __syncthreads();
-#pragma unroll
-      for (int k = 0; k < RPT; ++k)
-        if (pr[k] != 0xFFFFFFFFu) store_width(stage, k * T + threadIdx.x, c.width, x[k]);
-      __syncthreads();
-      for (int s = threadIdx.x; s < nvalid; s += T) {
-        unsigned p = psort[s];
-        int64_t g = (int64_t)gbase[p] + (s - (int)scan[p]);
-        if (g >= A.end[p]) continue;
-        int i = inv[s];
-        switch (c.width) {
-          case 1: ((uint8_t*)A.vals[v])[g] = stage[i]; break;
-          case 2: ((uint16_t*)A.vals[v])[g] = ((const uint16_t*)stage)[i]; break;
-          case 4: ((uint32_t*)A.vals[v])[g] = ((const uint32_t*)stage)[i]; break;
-          default: ((uint64_t*)A.vals[v])[g] = ((const uint64_t*)stage)[i]; break;
+      for (int u = 0; u < U; ++u) {
+        int s = sb + u * T + threadIdx.x;
+        g[u] = -1;
+        ii[u] = 0;
+        if (s < nvalid) {
+          unsigned p = psort[s];
+          int64_t gg = (int64_t)gbase[p] + (s - (int)scan[p]);
+          if (gg < A.end[p]) {
+            g[u] = gg;
+            ii[u] = inv[s];
+          }
         }
       }
-    }
-    if (any_bits) {
-      __syncthreads();
 #pragma unroll
-      for (int k = 0; k < RPT; ++k)
-        if (pr[k] != 0xFFFFFFFFu) stage[k * T + threadIdx.x] = (uint8_t)vb[k];
-      __syncthreads();
-      for (int s = threadIdx.x; s < nvalid; s += T) {
-        unsigned p = psort[s];
-        int64_t g = (int64_t)gbase[p] + (s - (int)scan[p]);
-        if (g < A.end[p]) A.bits[g] = stage[inv[s]];
+      for (int u = 0; u < U; ++u) {
+        if (g[u] < 0) continue;
+        if (KW == 1) A.keys[g[u]] = ((const uint64_t*)stage)[ii[u]];
+        else ((ulonglong2*)A.keys)[g[u]] = ((const ulonglong2*)stage)[ii[u]];
+      }
+      uint32_t vb[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) vb[u] = 0;
+#pragma unroll 1
+      for (int v = 0; v < P.num_vals; ++v) {
+        const ValCol& c = P.vals[v];
+        uint64_t x[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          x[u] = 0;
+          if (g[u] < 0) continue;
+          int64_t row = t0 + ii[u] + c.offset;
+          x[u] = load_bits(c.data, row, c.width);
+          if (any_bits && bit_valid(c.mask, row)) vb[u] |= 1u << v;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (g[u] >= 0) store_width(A.vals[v], g[u], c.width, x[u]);
+      }
+      if (any_bits) {
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (g[u] >= 0) A.bits[g[u]] = (uint8_t)vb[u];
       }
     }
     __syncthreads();
@@ -353,7 +363,7 @@ __global__ void __launch_bounds__(512, 1) k_part_aggregate(const __grid_constant
   __shared__ unsigned long long s_base;
   if (threadIdx.x == 0) s_new = 0;
   const int stride = G.stride;
-  const int nw = stride / 16;
+  const int nw = stride / 8;
   const uint64_t smask = (uint64_t)scap - 1;
   const int per = (scap + blockDim.x - 1) / blockDim.x;
   const bool have_bits = A.bits != nullptr;
@@ -366,7 +376,7 @@ __global__ void __launch_bounds__(512, 1) k_part_aggregate(const __grid_constant
     }
     for (int i = threadIdx.x; i < scap * nw; i += blockDim.x) {
       int s = i / nw;
-      *(uint4*)(smem + s * stride + (i - s * nw) * 16) = tmpl.w[i - s * nw];
+      *(unsigned long long*)(smem + s * stride + (i - s * nw) * 8) = tmpl.w[i - s * nw];
     }
     __syncthreads();
     const int p = s_part;
@@ -450,8 +460,8 @@ __global__ void __launch_bounds__(512, 1) k_part_aggregate(const __grid_constant
           atomicOr(D.overflow, 1u);
           break;
         }
-        uint4* dst = (uint4*)(D.T + o * stride);
-        for (int w = 0; w < nw; ++w) dst[w] = ((const uint4*)s)[w];
+        unsigned long long* dst = (unsigned long long*)(D.T + o * stride);
+        for (int w = 0; w < nw; ++w) dst[w] = ((const unsigned long long*)s)[w];
         ++o;
       }
     }
