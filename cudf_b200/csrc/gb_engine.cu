@@ -353,13 +353,21 @@ void build_plan(const std::vector<Column>& keys, int null_policy, const std::vec
   for (size_t v = 0; v < vk.size(); ++v) {
     ValCol& c = P.vals[v];
     c.acc_begin = c.acc_end = 0;
+    c.min_off = c.max_off = c.sq_off = -1;
+    c.sum_op = 0;
+    c.basic = 1;
     bool first = true;
     for (int a = 0; a < na; ++a)
       if (P.accs[a].col == v) {
         if (first) { c.acc_begin = (int16_t)a; first = false; }
         c.acc_end = (int16_t)(a + 1);
         uint8_t op = P.accs[a].op;
-        if (op == OP_SUM_I64 || op == OP_SUM_I32 || op == OP_SUM_F32 || op == OP_SUM_F64) c.sum_off = (int16_t)P.accs[a].off;
+        int16_t o = (int16_t)P.accs[a].off;
+        if (op == OP_SUM_I64 || op == OP_SUM_I32 || op == OP_SUM_F32 || op == OP_SUM_F64) { c.sum_off = o; c.sum_op = op; }
+        else if (op == OP_MIN_U32 || op == OP_MIN_U64) c.min_off = o;
+        else if (op == OP_MAX_U32 || op == OP_MAX_U64) c.max_off = o;
+        else if (op == OP_SQ_I64 || op == OP_SQ_F32 || op == OP_SQ_F64) c.sq_off = o;
+        else c.basic = 0;
       }
   }
   auto acc_for = [&](int v, uint8_t op) -> int16_t {
@@ -499,8 +507,10 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   }
 
   Scratch S(alloc, stream);
+  mark("begin");
   unsigned int* counters = (unsigned int*)S.get(4096);
   ck(cudaMemsetAsync(counters, 0, 4096, stream), "memset counters");
+  mark("counters");
   uint32_t* host = pinned();
   DevInfo dev = dev_info();
   SlotTemplate tmpl;
@@ -530,6 +540,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     k_sample_stats<<<dev.sms * 4, 256, 0, stream>>>(P, SR);
     st.kernels += 3;
     ck(cudaGetLastError(), "sample launch");
+    mark("sample launched");
     buckets.resize((size_t)1 << kBucketBits);
     ck(cudaMemcpyAsync(host, counters + 16, 16 * 4, cudaMemcpyDeviceToHost, stream), "sample d2h");
     ck(cudaMemcpyAsync(buckets.data(), bk, buckets.size() * 4, cudaMemcpyDeviceToHost, stream), "bucket d2h");
@@ -659,14 +670,8 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
         int grid = grid_for((const void*)kern, kScatterThreads, psmem, 0);
         kern<<<grid, kScatterThreads, psmem, stream>>>(P, A);
       };
-      int budget = dev.smem_optin - 4096;
-      if (P.key_words == 1) {
-        if ((int)part_scatter_smem(1, 32, nparts) <= budget) launch(k_part_scatter<1, 32>, 1, 32);
-        else launch(k_part_scatter<1, 16>, 1, 16);
-      } else {
-        if ((int)part_scatter_smem(2, 16, nparts) <= budget) launch(k_part_scatter<2, 16>, 2, 16);
-        else launch(k_part_scatter<2, 8>, 2, 8);
-      }
+      if (P.key_words == 1) launch(k_part_scatter<1, 16>, 1, 16);
+      else launch(k_part_scatter<2, 16>, 2, 16);
     }
     ++st.kernels;
     ck(cudaGetLastError(), "partition launch");

@@ -39,30 +39,26 @@ struct DenseRef {
   unsigned int* overflow;
 };
 
-// Pass 1.  Each CTA takes tiles of RPT*512 rows.  It first asks L2 for the
-// tile's value columns and masks (prefetch.global.L2, one per 128-byte line),
-// then loads the keys, counting-sorts the tile's rows by partition in shared
-// memory (keys staged there), reserves one run per (tile, partition) with a
-// global atomic, and finally writes every column in partition order: values
-// are gathered from L2 by the sorted row index, and consecutive threads write
-// consecutive positions of a partition's run, so stores leave in runs of
-// ~tile/nparts rows.
-// Shared memory: stage[tile * 8*KW] | inv u16[tile] | psort u16[tile] |
-//                hist u32[nparts] | scan u32[nparts] | gbase u64[nparts]
-constexpr int kScatterThreads = 512;
-
 __device__ __forceinline__ void prefetch_l2(const void* p)
 {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
+// Pass 1.  Each CTA takes tiles of RPT*256 rows.  A tile's rows are counting-
+// sorted by partition in shared memory (keys staged there, then each value
+// column in turn), so every (tile, partition) run leaves as one contiguous
+// write of ~tile/nparts rows instead of scattered 8-byte stores.  256 threads
+// and a 4K-row tile keep the footprint at ~64 KB so three CTAs share an SM;
+// each column's RPT loads per thread are issued back to back.
+// Shared memory: stage[tile * 8*KW] | inv u16[tile] | psort u16[tile] |
+//                hist u32[nparts] | scan u32[nparts] | gbase u64[nparts]
+constexpr int kScatterThreads = 256;
 template <int KW, int RPT>
-__global__ void __launch_bounds__(512, 1) k_part_scatter(const __grid_constant__ Plan P,
-                                                         const __grid_constant__ PartArgs A)
+__global__ void __launch_bounds__(256, 3) k_part_scatter(const __grid_constant__ Plan P,
+                                                      const __grid_constant__ PartArgs A)
 {
   constexpr int T = kScatterThreads;
   constexpr int TILE = RPT * T;
-  constexpr int U = 8;  // sorted rows per thread per gather batch
   extern __shared__ __align__(16) uint8_t sh[];
   uint8_t* stage = sh;
   uint16_t* inv = (uint16_t*)(sh + (size_t)TILE * 8 * KW);
@@ -78,23 +74,12 @@ __global__ void __launch_bounds__(512, 1) k_part_scatter(const __grid_constant__
   const int per = (A.nparts + T - 1) / T;  // partitions per thread in the scan
   for (int64_t t0 = (int64_t)blockIdx.x * TILE; t0 < n; t0 += (int64_t)gridDim.x * TILE) {
     const int cnt = (int)(n - t0 < (int64_t)TILE ? n - t0 : (int64_t)TILE);
-    // value columns and masks of this tile into L2 while the keys are sorted
-    for (int v = 0; v < P.num_vals; ++v) {
-      const ValCol& c = P.vals[v];
-      const uint8_t* base = (const uint8_t*)c.data + (t0 + c.offset) * c.width;
-      int64_t bytes = (int64_t)cnt * c.width;
-      for (int64_t o = (int64_t)threadIdx.x * 128; o < bytes; o += (int64_t)T * 128) prefetch_l2(base + o);
-      if (c.mask) {
-        int64_t w = (t0 + c.offset) / 32 + (int64_t)threadIdx.x * 32;
-        if (w <= (t0 + c.offset + cnt - 1) / 32) prefetch_l2(c.mask + w);
-      }
-    }
     for (int i = threadIdx.x; i < A.nparts; i += T) hist[i] = 0;
     __syncthreads();
     // A: keys -> stage, partition ids and ranks
     uint32_t pr[RPT];
-    if (KW == 1 && P.num_keys == 1 && !P.keys[0].mask && P.keys[0].width == 8 && P.keys[0].cat != CAT_F64) {
-      // one plain 64-bit key: all RPT loads in flight first
+    if (P.num_keys == 1 && !P.keys[0].mask && P.keys[0].width == 8 && P.keys[0].cat != CAT_F64) {
+      // one plain 64-bit key: load all RPT keys first
       const unsigned long long* kd = (const unsigned long long*)P.keys[0].data + P.keys[0].offset;
       uint64_t kk[RPT];
 #pragma unroll
@@ -157,53 +142,63 @@ __global__ void __launch_bounds__(512, 1) k_part_scatter(const __grid_constant__
     }
     __syncthreads();
     const int nvalid = (int)s_valid;
-    // D: every column out in partition order, U sorted rows per thread at a time
-    for (int sb = 0; sb < nvalid; sb += U * T) {
-      int64_t g[U];
-      int ii[U];
+    // D: keys out
+    for (int s = threadIdx.x; s < nvalid; s += T) {
+      unsigned p = psort[s];
+      int64_t g = (int64_t)gbase[p] + (s - (int)scan[p]);
+      if (g >= A.end[p]) continue;
+      if (KW == 1) A.keys[g] = ((const uint64_t*)stage)[inv[s]];
+      else ((ulonglong2*)A.keys)[g] = ((const ulonglong2*)stage)[inv[s]];
+    }
+    // E: each value column through the stage
+    uint32_t vb[RPT];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        int s = sb + u * T + threadIdx.x;
-        g[u] = -1;
-        ii[u] = 0;
-        if (s < nvalid) {
-          unsigned p = psort[s];
-          int64_t gg = (int64_t)gbase[p] + (s - (int)scan[p]);
-          if (gg < A.end[p]) {
-            g[u] = gg;
-            ii[u] = inv[s];
-          }
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (g[u] < 0) continue;
-        if (KW == 1) A.keys[g[u]] = ((const uint64_t*)stage)[ii[u]];
-        else ((ulonglong2*)A.keys)[g[u]] = ((const ulonglong2*)stage)[ii[u]];
-      }
-      uint32_t vb[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) vb[u] = 0;
+    for (int k = 0; k < RPT; ++k) vb[k] = 0;
 #pragma unroll 1
-      for (int v = 0; v < P.num_vals; ++v) {
-        const ValCol& c = P.vals[v];
-        uint64_t x[U];
+    for (int v = 0; v < P.num_vals; ++v) {
+      const ValCol& c = P.vals[v];
+      uint64_t x[RPT];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-          x[u] = 0;
-          if (g[u] < 0) continue;
-          int64_t row = t0 + ii[u] + c.offset;
-          x[u] = load_bits(c.data, row, c.width);
-          if (any_bits && bit_valid(c.mask, row)) vb[u] |= 1u << v;
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-          if (g[u] >= 0) store_width(A.vals[v], g[u], c.width, x[u]);
+      for (int k = 0; k < RPT; ++k) {
+        int i = k * T + threadIdx.x;
+        x[k] = pr[k] != 0xFFFFFFFFu ? load_bits(c.data, t0 + i + c.offset, c.width) : 0;
       }
-      if (any_bits) {
+      if (any_bits && c.mask) {
 #pragma unroll
-        for (int u = 0; u < U; ++u)
-          if (g[u] >= 0) A.bits[g[u]] = (uint8_t)vb[u];
+        for (int k = 0; k < RPT; ++k)
+          if (pr[k] != 0xFFFFFFFFu && bit_valid(c.mask, t0 + k * T + threadIdx.x + c.offset)) vb[k] |= 1u << v;
+      } else if (any_bits) {
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) vb[k] |= 1u << v;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < RPT; ++k)
+        if (pr[k] != 0xFFFFFFFFu) store_width(stage, k * T + threadIdx.x, c.width, x[k]);
+      __syncthreads();
+      for (int s = threadIdx.x; s < nvalid; s += T) {
+        unsigned p = psort[s];
+        int64_t g = (int64_t)gbase[p] + (s - (int)scan[p]);
+        if (g >= A.end[p]) continue;
+        int i = inv[s];
+        switch (c.width) {
+          case 1: ((uint8_t*)A.vals[v])[g] = stage[i]; break;
+          case 2: ((uint16_t*)A.vals[v])[g] = ((const uint16_t*)stage)[i]; break;
+          case 4: ((uint32_t*)A.vals[v])[g] = ((const uint32_t*)stage)[i]; break;
+          default: ((uint64_t*)A.vals[v])[g] = ((const uint64_t*)stage)[i]; break;
+        }
+      }
+    }
+    if (any_bits) {
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < RPT; ++k)
+        if (pr[k] != 0xFFFFFFFFu) stage[k * T + threadIdx.x] = (uint8_t)vb[k];
+      __syncthreads();
+      for (int s = threadIdx.x; s < nvalid; s += T) {
+        unsigned p = psort[s];
+        int64_t g = (int64_t)gbase[p] + (s - (int)scan[p]);
+        if (g < A.end[p]) A.bits[g] = stage[inv[s]];
       }
     }
     __syncthreads();
@@ -333,6 +328,51 @@ __device__ __forceinline__ void sapply(const Plan& P, const ValCol& c, uint32_t 
   }
 }
 
+// Same as sapply for a column whose accumulators are only SUM/MIN/MAX/sum of
+// squares: the value is converted once and each accumulator is a fixed
+// offset, without the per-accumulator dispatch.
+__device__ __forceinline__ void sapply_basic(const ValCol& c, uint32_t sa, uint64_t bits)
+{
+  const uint8_t cat = c.cat;
+  int64_t iv = 0;
+  float f = 0.f;
+  double d = 0.0;
+  if (cat == CAT_F32) { f = __uint_as_float((uint32_t)bits); d = f; }
+  else if (cat == CAT_F64) d = __longlong_as_double((long long)bits);
+  else if (cat == CAT_SIGNED) iv = sign_extend(bits, c.width);
+  else if (cat == CAT_BOOL) iv = bits != 0;
+  else iv = (int64_t)bits;
+  switch (c.sum_op) {
+    case OP_SUM_I64: sred_add_u64(sa + c.sum_off, (uint64_t)iv); break;
+    case OP_SUM_I32: sred_add_u32(sa + c.sum_off, (uint32_t)iv); break;
+    case OP_SUM_F32: sred_add_f32(sa + c.sum_off, f); break;
+    case OP_SUM_F64: sred_add_f64(sa + c.sum_off, d); break;
+    default: break;
+  }
+  if (c.min_off >= 0 || c.max_off >= 0) {
+    if (c.width == 8) {
+      uint64_t lo, hi;
+      if (cat == CAT_F64) { lo = ord64_f(d, true); hi = ord64_f(d, false); }
+      else if (cat == CAT_UNSIGNED) lo = hi = bits;
+      else lo = hi = (uint64_t)iv ^ 0x8000000000000000ull;
+      if (c.min_off >= 0 && lo < sld_u64(sa + c.min_off)) sred_min_u64(sa + c.min_off, lo);
+      if (c.max_off >= 0 && hi > sld_u64(sa + c.max_off)) sred_max_u64(sa + c.max_off, hi);
+    } else {
+      uint32_t lo, hi;
+      if (cat == CAT_F32) { lo = ord32_f(f, true); hi = ord32_f(f, false); }
+      else if (cat == CAT_UNSIGNED || cat == CAT_BOOL) lo = hi = (uint32_t)iv;
+      else lo = hi = (uint32_t)(int32_t)iv ^ 0x80000000u;
+      if (c.min_off >= 0 && lo < sld_u32(sa + c.min_off)) sred_min_u32(sa + c.min_off, lo);
+      if (c.max_off >= 0 && hi > sld_u32(sa + c.max_off)) sred_max_u32(sa + c.max_off, hi);
+    }
+  }
+  if (c.sq_off >= 0) {
+    if (cat == CAT_F32) sred_add_f32(sa + c.sq_off, f * f);
+    else if (cat == CAT_F64) sred_add_f64(sa + c.sq_off, d * d);
+    else sred_add_u64(sa + c.sq_off, (uint64_t)iv * (uint64_t)iv);
+  }
+}
+
 // A row whose key did not fit the shared table: global table, generic update.
 __device__ __noinline__ void spill_row(const Plan& P2, const TableRef& G, uint64_t w0, uint64_t w1,
                                        uint64_t h, int64_t r, unsigned int* s_new)
@@ -384,6 +424,21 @@ __global__ void __launch_bounds__(512, 1) k_part_aggregate(const __grid_constant
     const int64_t b = A.base[p];
     const int64_t e = min((int64_t)A.cursor[p], A.end[p]);
     for (int64_t r0 = b; r0 < e; r0 += (int64_t)R * blockDim.x) {
+      // the step after the next one into L2 (one prefetch per 128-byte line per array)
+      {
+        const int64_t n0 = r0 + 2 * (int64_t)R * blockDim.x;
+        const int64_t n1 = min(e, n0 + (int64_t)R * blockDim.x);
+        if (n0 < n1) {
+          int t = threadIdx.x;
+          int64_t kb = (n1 - n0) * 8 * P2.key_words;
+          if ((int64_t)t * 128 < kb) prefetch_l2((const uint8_t*)(P2.packed_keys + n0 * P2.key_words) + (int64_t)t * 128);
+          for (int v = 0; v < P2.num_vals; ++v) {
+            int64_t vbytes = (n1 - n0) * P2.vals[v].width;
+            if ((int64_t)t * 128 < vbytes) prefetch_l2((const uint8_t*)P2.vals[v].data + n0 * P2.vals[v].width + (int64_t)t * 128);
+          }
+          if (have_bits && (int64_t)t * 128 < n1 - n0) prefetch_l2(A.bits + n0 + (int64_t)t * 128);
+        }
+      }
       uint64_t k0[R], k1[R];
       uint32_t vb[R], sa[R];
 #pragma unroll
@@ -433,7 +488,8 @@ __global__ void __launch_bounds__(512, 1) k_part_aggregate(const __grid_constant
             if (c.nulls_off >= 0) sred_add_u32(sa[j] + c.nulls_off, 1u);
             continue;
           }
-          sapply(P2, c, sa[j], x[j]);
+          if (c.basic) sapply_basic(c, sa[j], x[j]);
+          else sapply(P2, c, sa[j], x[j]);
         }
       }
     }

@@ -85,6 +85,13 @@ struct ValCol {
   int32_t ddof;           // VARIANCE/STD ddof (one per column; requests with another ddof get a copy)
   const uint8_t* bits;    // partitioned rows: validity byte per row (bit `bit`), else null
   int32_t bit;
+  // the column's accumulators in closed form, for kernels that skip the
+  // per-accumulator interpreter: offsets (-1 when absent) and the sum op
+  int16_t min_off;
+  int16_t max_off;
+  int16_t sq_off;
+  uint8_t sum_op;         // OP_SUM_* or 0
+  uint8_t basic;          // 1 when every accumulator is a SUM, MIN, MAX or sum of squares
 };
 
 struct Acc {
