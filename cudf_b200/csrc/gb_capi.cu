@@ -154,7 +154,7 @@ int gb_set_tuning(gb_handle* h, const gb_tuning* t)
     if (!h || !t) throw gb::Error(gb::ERR_LOGIC, "null handle or tuning");
     gb::Options& o = h->opt;
     if (t->block > 0) {
-      if (t->block % 32 || t->block > 512) throw gb::Error(gb::ERR_LOGIC, "block must be a multiple of 32, <= 512");
+      if (t->block % 32 || t->block > 1024) throw gb::Error(gb::ERR_LOGIC, "block must be a multiple of 32, <= 1024");
       o.block = t->block;
     }
     if (t->blocks_per_sm >= 0) o.blocks_per_sm = t->blocks_per_sm;

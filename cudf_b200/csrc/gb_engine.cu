@@ -698,13 +698,14 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       G = TableRef{T, spill_cap - 1, P.slot_bytes, P.key_words, counters};
       DenseRef D{dense, dcap, (unsigned long long*)(counters + 10), counters + 6};
       size_t sm2 = (size_t)scap2 * P.slot_bytes;
-      auto launch2 = [&](auto kern) {
+      auto launch2 = [&](auto kern, int nt) {
         ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2), "attr");
-        int grid = grid_for((const void*)kern, 512, sm2, 0);
+        int grid = grid_for((const void*)kern, nt, sm2, 0);
         grid = std::min(grid, nparts);
-        kern<<<grid, 512, sm2, stream>>>(P2, A, G, D, scap2, sfill2, tmpl);
+        kern<<<grid, nt, sm2, stream>>>(P2, A, G, D, scap2, sfill2, tmpl);
       };
-      launch2(k_part_aggregate<4>);
+      if (P.num_vals <= 4 && opt.block >= 1024) launch2(k_part_aggregate<1, 1024, 4>, 1024);
+      else launch2(k_part_aggregate<2, 512, 8>, 512);
       if (opt.profile) ck(cudaEventRecord(events()[1], stream), "event");
       k_finish_count<<<1, 1, 0, stream>>>(P, G);
       st.kernels += 3;
@@ -750,7 +751,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       k_init_slots<<<dev.sms * 8, 256, 0, stream>>>(T, (int64_t)cap + 1, P.slot_bytes, tmpl);
       ck(cudaMemsetAsync(counters, 0, 16, stream), "memset counters");
       G = TableRef{T, cap - 1, P.slot_bytes, P.key_words, counters};
-      int block = opt.block;
+      int block = std::min(opt.block, 512);
       if (opt.profile) ck(cudaEventRecord(events()[0], stream), "event");
       if (mode == 1) {
         size_t sm = (size_t)scap * P.slot_bytes;

@@ -68,7 +68,7 @@ struct Result {
 
 // Engine tunables (an autotuner picks these per size bucket).
 struct Options {
-  int block = 512;             // threads per CTA of the aggregation kernel
+  int block = 1024;            // threads per CTA (partitioned pass 2; other kernels use at most 512)
   int blocks_per_sm = 0;       // 0 = occupancy limited
   int smem_bytes = 96 * 1024;  // shared-memory table bytes per CTA (0 disables the smem stage)
   double smem_fill = 0.5;      // fraction of smem slots a CTA may claim

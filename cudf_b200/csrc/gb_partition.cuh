@@ -253,14 +253,14 @@ __device__ __forceinline__ uint8_t* smem_slot(uint8_t* smem, int stride, uint64_
 }
 
 // ---- explicit shared-memory operations (32-bit shared-window addresses) ----
-__device__ __forceinline__ void sred_add_u32(uint32_t a, uint32_t v) { asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory"); }
-__device__ __forceinline__ void sred_add_u64(uint32_t a, uint64_t v) { asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); }
-__device__ __forceinline__ void sred_add_f32(uint32_t a, float v) { asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory"); }
-__device__ __forceinline__ void sred_add_f64(uint32_t a, double v) { asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory"); }
-__device__ __forceinline__ void sred_min_u32(uint32_t a, uint32_t v) { asm volatile("red.shared.min.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory"); }
-__device__ __forceinline__ void sred_max_u32(uint32_t a, uint32_t v) { asm volatile("red.shared.max.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory"); }
-__device__ __forceinline__ void sred_min_u64(uint32_t a, uint64_t v) { asm volatile("red.shared.min.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); }
-__device__ __forceinline__ void sred_max_u64(uint32_t a, uint64_t v) { asm volatile("red.shared.max.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); }
+__device__ __forceinline__ void sred_add_u32(uint32_t a, uint32_t v) { asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(a), "r"(v)); }
+__device__ __forceinline__ void sred_add_u64(uint32_t a, uint64_t v) { asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a), "l"(v)); }
+__device__ __forceinline__ void sred_add_f32(uint32_t a, float v) { asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(v)); }
+__device__ __forceinline__ void sred_add_f64(uint32_t a, double v) { asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(a), "d"(v)); }
+__device__ __forceinline__ void sred_min_u32(uint32_t a, uint32_t v) { asm volatile("red.shared.min.u32 [%0], %1;" ::"r"(a), "r"(v)); }
+__device__ __forceinline__ void sred_max_u32(uint32_t a, uint32_t v) { asm volatile("red.shared.max.u32 [%0], %1;" ::"r"(a), "r"(v)); }
+__device__ __forceinline__ void sred_min_u64(uint32_t a, uint64_t v) { asm volatile("red.shared.min.u64 [%0], %1;" ::"r"(a), "l"(v)); }
+__device__ __forceinline__ void sred_max_u64(uint32_t a, uint64_t v) { asm volatile("red.shared.max.u64 [%0], %1;" ::"r"(a), "l"(v)); }
 __device__ __forceinline__ uint32_t sld_u32(uint32_t a)
 {
   uint32_t v;
@@ -282,7 +282,7 @@ __device__ __forceinline__ bool part_op_ok(uint8_t op)
 }
 
 // Applies one valid value (raw bits) of column c to a shared slot at `sa`.
-__device__ __forceinline__ void sapply(const Plan& P, const ValCol& c, uint32_t sa, uint64_t bits)
+__device__ __noinline__ void sapply(const Plan& P, const ValCol& c, uint32_t sa, uint64_t bits)
 {
   int64_t iv = 0;
   float f = 0.f;
@@ -355,15 +355,15 @@ __device__ __forceinline__ void sapply_basic(const ValCol& c, uint32_t sa, uint6
       if (cat == CAT_F64) { lo = ord64_f(d, true); hi = ord64_f(d, false); }
       else if (cat == CAT_UNSIGNED) lo = hi = bits;
       else lo = hi = (uint64_t)iv ^ 0x8000000000000000ull;
-      if (c.min_off >= 0 && lo < sld_u64(sa + c.min_off)) sred_min_u64(sa + c.min_off, lo);
-      if (c.max_off >= 0 && hi > sld_u64(sa + c.max_off)) sred_max_u64(sa + c.max_off, hi);
+      if (c.min_off >= 0) sred_min_u64(sa + c.min_off, lo);
+      if (c.max_off >= 0) sred_max_u64(sa + c.max_off, hi);
     } else {
       uint32_t lo, hi;
       if (cat == CAT_F32) { lo = ord32_f(f, true); hi = ord32_f(f, false); }
       else if (cat == CAT_UNSIGNED || cat == CAT_BOOL) lo = hi = (uint32_t)iv;
       else lo = hi = (uint32_t)(int32_t)iv ^ 0x80000000u;
-      if (c.min_off >= 0 && lo < sld_u32(sa + c.min_off)) sred_min_u32(sa + c.min_off, lo);
-      if (c.max_off >= 0 && hi > sld_u32(sa + c.max_off)) sred_max_u32(sa + c.max_off, hi);
+      if (c.min_off >= 0) sred_min_u32(sa + c.min_off, lo);
+      if (c.max_off >= 0) sred_max_u32(sa + c.max_off, hi);
     }
   }
   if (c.sq_off >= 0) {
@@ -385,19 +385,81 @@ __device__ __noinline__ void spill_row(const Plan& P2, const TableRef& G, uint64
   update_slot(P2, G.T + gi * (int64_t)G.stride, r);
 }
 
+// ---- pass 2 ----
+// Per-partition prologue: claim a partition, reset the shared table.  Returns
+// the partition id (>= nparts: no work left).
+template <int NT>
+__device__ __forceinline__ int p2_claim(const PartArgs& A, uint8_t* smem, int scap, int nw,
+                                        const SlotTemplate& tmpl, int* s_part, unsigned int* s_used,
+                                        unsigned int* s_spill)
+{
+  if (threadIdx.x == 0) {
+    *s_part = (int)atomicAdd(A.counters + 8, 1u);
+    *s_used = 0;
+    *s_spill = 0;
+  }
+  for (int i = threadIdx.x; i < scap * nw; i += NT) {
+    int s = i / nw;
+    *(unsigned long long*)(smem + (size_t)s * nw * 8 + (i - s * nw) * 8) = tmpl.w[i - s * nw];
+  }
+  __syncthreads();
+  return *s_part;
+}
+
+// Per-partition epilogue: the partition's groups leave as dense slots, or are
+// merged into the global spill table when some of its rows went there.
+template <int NT, typename ScanT>
+__device__ __forceinline__ void p2_flush(const Plan& P2, const TableRef& G, const DenseRef& D,
+                                         const uint8_t* smem, int scap, bool spilled,
+                                         typename ScanT::TempStorage& scan_tmp,
+                                         unsigned long long* s_base, unsigned int* s_new)
+{
+  const int stride = G.stride;
+  const int nw = stride / 8;
+  if (spilled) {
+    for (int i = threadIdx.x; i < scap; i += NT) {
+      const uint8_t* s = smem + i * stride;
+      if (slot_occupied(P2, s, false)) merge_slot(P2, G, s, s_new);
+    }
+    return;
+  }
+  const int per = (scap + NT - 1) / NT;
+  int first = threadIdx.x * per;
+  unsigned mine = 0;
+  for (int i = first; i < min(first + per, scap); ++i) mine += slot_occupied(P2, smem + i * stride, false);
+  unsigned off, total;
+  ScanT(scan_tmp).ExclusiveSum(mine, off, total);
+  if (threadIdx.x == 0) *s_base = total ? atomicAdd(D.count, (unsigned long long)total) : 0ull;
+  __syncthreads();
+  unsigned long long o = *s_base + off;
+  for (int i = first; i < min(first + per, scap); ++i) {
+    const uint8_t* s = smem + i * stride;
+    if (!slot_occupied(P2, s, false)) continue;
+    if ((int64_t)o >= D.cap) {
+      atomicOr(D.overflow, 1u);
+      break;
+    }
+    unsigned long long* dst = (unsigned long long*)(D.T + o * stride);
+    for (int w = 0; w < nw; ++w) dst[w] = ((const unsigned long long*)s)[w];
+    ++o;
+  }
+}
+
 // Pass 2.  P2 is the plan with value columns redirected to the partitioned
-// arrays (offset 0, `bits` validity) and packed_keys set.  R rows per thread
-// per step: keys first, then the shared slot of each, then column by column
-// the values (R loads in flight) and their shared-memory updates.
-template <int R>
-__global__ void __launch_bounds__(512, 1) k_part_aggregate(const __grid_constant__ Plan P2,
-                                                           const __grid_constant__ PartArgs A,
-                                                           TableRef G, DenseRef D, int scap, int sfill,
-                                                           const __grid_constant__ SlotTemplate tmpl)
+// arrays (offset 0, `bits` validity) and packed_keys set.  One CTA owns a
+// partition at a time and aggregates it in a shared-memory table.  The row
+// loop is software-pipelined: while step t's rows are placed in the table,
+// step t's values (every column) and step t+1's keys are already in flight,
+// and step t+2 is prefetched into L2.  MAXV bounds the value columns.
+template <int R, int NT, int MAXV>
+__global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant__ Plan P2,
+                                                          const __grid_constant__ PartArgs A,
+                                                          TableRef G, DenseRef D, int scap, int sfill,
+                                                          const __grid_constant__ SlotTemplate tmpl)
 {
   extern __shared__ __align__(16) uint8_t smem[];
-  using Scan = cub::BlockScan<unsigned, 512>;
-  __shared__ typename Scan::TempStorage scan_tmp;
+  using ScanT = cub::BlockScan<unsigned, NT>;
+  __shared__ typename ScanT::TempStorage scan_tmp;
   __shared__ int s_part;
   __shared__ unsigned int s_used, s_spill, s_new;
   __shared__ unsigned long long s_base;
@@ -405,122 +467,109 @@ __global__ void __launch_bounds__(512, 1) k_part_aggregate(const __grid_constant
   const int stride = G.stride;
   const int nw = stride / 8;
   const uint64_t smask = (uint64_t)scap - 1;
-  const int per = (scap + blockDim.x - 1) / blockDim.x;
   const bool have_bits = A.bits != nullptr;
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
+  const int kw = P2.key_words;
+  const int nv = P2.num_vals;
   for (;;) {
-    if (threadIdx.x == 0) {
-      s_part = (int)atomicAdd(A.counters + 8, 1u);
-      s_used = 0;
-      s_spill = 0;
-    }
-    for (int i = threadIdx.x; i < scap * nw; i += blockDim.x) {
-      int s = i / nw;
-      *(unsigned long long*)(smem + s * stride + (i - s * nw) * 8) = tmpl.w[i - s * nw];
-    }
-    __syncthreads();
-    const int p = s_part;
+    const int p = p2_claim<NT>(A, smem, scap, nw, tmpl, &s_part, &s_used, &s_spill);
     if (p >= A.nparts) break;
     const int64_t b = A.base[p];
     const int64_t e = min((int64_t)A.cursor[p], A.end[p]);
-    for (int64_t r0 = b; r0 < e; r0 += (int64_t)R * blockDim.x) {
-      // the step after the next one into L2 (one prefetch per 128-byte line per array)
-      {
-        const int64_t n0 = r0 + 2 * (int64_t)R * blockDim.x;
-        const int64_t n1 = min(e, n0 + (int64_t)R * blockDim.x);
-        if (n0 < n1) {
-          int t = threadIdx.x;
-          int64_t kb = (n1 - n0) * 8 * P2.key_words;
-          if ((int64_t)t * 128 < kb) prefetch_l2((const uint8_t*)(P2.packed_keys + n0 * P2.key_words) + (int64_t)t * 128);
-          for (int v = 0; v < P2.num_vals; ++v) {
-            int64_t vbytes = (n1 - n0) * P2.vals[v].width;
-            if ((int64_t)t * 128 < vbytes) prefetch_l2((const uint8_t*)P2.vals[v].data + n0 * P2.vals[v].width + (int64_t)t * 128);
-          }
-          if (have_bits && (int64_t)t * 128 < n1 - n0) prefetch_l2(A.bits + n0 + (int64_t)t * 128);
-        }
-      }
-      uint64_t k0[R], k1[R];
-      uint32_t vb[R], sa[R];
+    constexpr int64_t STEP = (int64_t)R * NT;
+    auto load_keys = [&](int64_t r0, uint64_t (&k0)[R], uint64_t (&k1)[R], uint32_t (&vb)[R]) {
 #pragma unroll
       for (int j = 0; j < R; ++j) {
-        int64_t r = r0 + (int64_t)j * blockDim.x + threadIdx.x;
+        int64_t r = r0 + (int64_t)j * NT + threadIdx.x;
         k0[j] = kEmpty;
         k1[j] = 0;
         vb[j] = 0xFFFFFFFFu;
         if (r < e) {
-          if (P2.key_words == 1) k0[j] = P2.packed_keys[r];
+          if (kw == 1) k0[j] = __ldg(P2.packed_keys + r);
           else {
-            ulonglong2 kk = *(const ulonglong2*)(P2.packed_keys + 2 * r);
+            ulonglong2 kk = __ldg((const ulonglong2*)(P2.packed_keys + 2 * r));
             k0[j] = kk.x;
             k1[j] = kk.y;
           }
-          if (have_bits) vb[j] = A.bits[r];
+          if (have_bits) vb[j] = __ldg(A.bits + r);
         }
       }
+    };
+    uint64_t k0[R], k1[R];
+    uint32_t vb[R];
+    load_keys(b, k0, k1, vb);
+    for (int64_t r0 = b; r0 < e; r0 += STEP) {
+      // step t+2 into L2
+      {
+        const int64_t n0 = r0 + 2 * STEP;
+        const int64_t n1 = min(e, n0 + STEP);
+        if (n0 < n1) {
+          const int64_t t = threadIdx.x;
+          if (t * 128 < (n1 - n0) * 8 * kw) prefetch_l2((const uint8_t*)(P2.packed_keys + n0 * kw) + t * 128);
+#pragma unroll
+          for (int v = 0; v < MAXV; ++v) {
+            if (v >= nv) break;
+            if (t * 128 < (n1 - n0) * P2.vals[v].width)
+              prefetch_l2((const uint8_t*)P2.vals[v].data + n0 * P2.vals[v].width + t * 128);
+          }
+          if (have_bits && t * 128 < n1 - n0) prefetch_l2(A.bits + n0 + t * 128);
+        }
+      }
+      // place this step's rows
+      uint32_t sa[R];
 #pragma unroll
       for (int j = 0; j < R; ++j) {
-        int64_t r = r0 + (int64_t)j * blockDim.x + threadIdx.x;
+        int64_t r = r0 + (int64_t)j * NT + threadIdx.x;
         sa[j] = 0;
         if (r >= e) continue;
-        uint64_t h = hash_key(k0[j], k1[j], P2.key_words);
-        uint8_t* slot = smem_slot(smem, stride, smask, sfill, &s_used, P2.key_words, k0[j], k1[j], h);
+        uint64_t h = hash_key(k0[j], k1[j], kw);
+        uint8_t* slot = smem_slot(smem, stride, smask, sfill, &s_used, kw, k0[j], k1[j], h);
         if (slot == nullptr) {
           s_spill = 1;
           spill_row(P2, G, k0[j], k1[j], h, r, &s_new);
           continue;
         }
         sa[j] = sbase + (uint32_t)(slot - smem);
-        sred_add_u32(sa[j] + P2.rows_off, 1u);
       }
-#pragma unroll 1
-      for (int v = 0; v < P2.num_vals; ++v) {
-        const ValCol& c = P2.vals[v];
-        uint64_t x[R];
+      // this step's values and the next step's keys in flight together
+      uint64_t x[R][MAXV];
 #pragma unroll
-        for (int j = 0; j < R; ++j) {
-          int64_t r = r0 + (int64_t)j * blockDim.x + threadIdx.x;
-          x[j] = (sa[j] && ((vb[j] >> v) & 1)) ? load_bits(c.data, r, c.width) : 0;
+      for (int j = 0; j < R; ++j) {
+        int64_t r = r0 + (int64_t)j * NT + threadIdx.x;
+#pragma unroll
+        for (int v = 0; v < MAXV; ++v) {
+          x[j][v] = 0;
+          if (v < nv && sa[j] && ((vb[j] >> v) & 1)) x[j][v] = load_bits(P2.vals[v].data, r, P2.vals[v].width);
         }
+      }
+      uint64_t nk0[R], nk1[R];
+      uint32_t nvb[R];
+      load_keys(r0 + STEP, nk0, nk1, nvb);
 #pragma unroll
-        for (int j = 0; j < R; ++j) {
-          if (!sa[j]) continue;
+      for (int j = 0; j < R; ++j) {
+        if (!sa[j]) continue;
+        sred_add_u32(sa[j] + P2.rows_off, 1u);
+#pragma unroll
+        for (int v = 0; v < MAXV; ++v) {
+          if (v >= nv) break;
+          const ValCol& c = P2.vals[v];
           if (!((vb[j] >> v) & 1)) {
             if (c.nulls_off >= 0) sred_add_u32(sa[j] + c.nulls_off, 1u);
             continue;
           }
-          if (c.basic) sapply_basic(c, sa[j], x[j]);
-          else sapply(P2, c, sa[j], x[j]);
+          if (c.basic) sapply_basic(c, sa[j], x[j][v]);
+          else sapply(P2, c, sa[j], x[j][v]);
         }
+      }
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        k0[j] = nk0[j];
+        k1[j] = nk1[j];
+        vb[j] = nvb[j];
       }
     }
     __syncthreads();
-    if (s_spill) {
-      for (int i = threadIdx.x; i < scap; i += blockDim.x) {
-        const uint8_t* s = smem + i * stride;
-        if (slot_occupied(P2, s, false)) merge_slot(P2, G, s, &s_new);
-      }
-    } else {
-      // copy this partition's groups out as dense slots, in slot order
-      int first = threadIdx.x * per;
-      unsigned mine = 0;
-      for (int i = first; i < min(first + per, scap); ++i) mine += slot_occupied(P2, smem + i * stride, false);
-      unsigned off, total;
-      Scan(scan_tmp).ExclusiveSum(mine, off, total);
-      if (threadIdx.x == 0) s_base = total ? atomicAdd(D.count, (unsigned long long)total) : 0ull;
-      __syncthreads();
-      unsigned long long o = s_base + off;
-      for (int i = first; i < min(first + per, scap); ++i) {
-        const uint8_t* s = smem + i * stride;
-        if (!slot_occupied(P2, s, false)) continue;
-        if ((int64_t)o >= D.cap) {
-          atomicOr(D.overflow, 1u);
-          break;
-        }
-        unsigned long long* dst = (unsigned long long*)(D.T + o * stride);
-        for (int w = 0; w < nw; ++w) dst[w] = ((const unsigned long long*)s)[w];
-        ++o;
-      }
-    }
+    p2_flush<NT, ScanT>(P2, G, D, smem, scap, s_spill != 0, scan_tmp, &s_base, &s_new);
     __syncthreads();
   }
   if (threadIdx.x == 0 && s_new) atomicAdd(G.counters, s_new);
