@@ -88,6 +88,10 @@ SIGNATURES = {
     "gb_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GbTuning)]),
     "gb_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GbStats)]),
     "gb_version": (ctypes.c_char_p, []),
+    "gb_aggregate_noalloc": (ctypes.c_int, [ctypes.POINTER(GbColumn), ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.POINTER(GbRequest), ctypes.c_int32, ctypes.c_int64,
+                                            ctypes.POINTER(GbOutColumn), ctypes.POINTER(GbOutColumn),
+                                            ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p]),
 }
 
 

@@ -60,6 +60,10 @@ gb_out_column to_out(const gb::OutColumn& c)
 }
 }  // namespace
 
+namespace gb {
+void set_last_error(const std::string& msg) { t_err = msg; }
+}  // namespace gb
+
 struct gb_handle {
   std::vector<gb::Column> keys;
   int null_policy;

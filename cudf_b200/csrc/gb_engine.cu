@@ -855,3 +855,115 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
 }
 
 }  // namespace gb
+
+namespace gb {
+
+// Global-table aggregation whose hash table and counters live in `scratch`
+// (caller-owned device memory) and whose results go to caller-owned columns:
+// the path makes no device or pinned-host allocation.  Counters are read back
+// with pageable copies.  Returns the number of groups.
+int64_t aggregate_into_scratch(const std::vector<Column>& keys, int null_policy,
+                               const std::vector<Request>& reqs, cudaStream_t stream, void* scratch,
+                               size_t scratch_bytes, int64_t max_groups,
+                               std::vector<OutColumn>& out_keys, std::vector<OutColumn>& out_results)
+{
+  Plan P;
+  std::vector<int> out_types;
+  build_plan(keys, null_policy, reqs, P, out_types);
+  if (max_groups < 0) throw Error(ERR_LOGIC, "max_groups must be >= 0");
+  if (out_keys.size() != (size_t)P.num_keys || out_results.size() != (size_t)P.num_outs)
+    throw Error(ERR_LOGIC, "output column count does not match the keys and requests");
+  for (int k = 0; k < P.num_keys; ++k) {
+    OutColumn& o = out_keys[k];
+    o.type_id = keys[k].type_id;
+    if (max_groups > 0 && !o.data) throw Error(ERR_LOGIC, "output key column without a data buffer");
+    if (keys[k].mask && max_groups > 0 && !o.mask) throw Error(ERR_LOGIC, "nullable output key column without a mask buffer");
+    if (!keys[k].mask) o.mask = nullptr;
+  }
+  for (int j = 0; j < P.num_outs; ++j) {
+    OutColumn& o = out_results[j];
+    o.type_id = out_types[j];
+    if (max_groups > 0 && !o.data) throw Error(ERR_LOGIC, "output result column without a data buffer");
+    if (P.outs[j].nullable && max_groups > 0 && !o.mask) throw Error(ERR_LOGIC, "nullable output result column without a mask buffer");
+    if (!P.outs[j].nullable) o.mask = nullptr;
+  }
+  const int64_t n = P.num_rows;
+  const uint64_t cap = next_pow2((uint64_t)std::max<int64_t>(64, 2 * max_groups));
+  const size_t need = 4096 + (size_t)(cap + 1) * P.slot_bytes;
+  if (need > scratch_bytes)
+    throw Error(ERR_LOGIC, "max_groups " + std::to_string(max_groups) + " with this plan's " +
+                               std::to_string(P.slot_bytes) + "-byte slots needs " + std::to_string(need) +
+                               " bytes of table; the allocation-free entry point has " +
+                               std::to_string(scratch_bytes));
+  unsigned int* counters = (unsigned int*)scratch;
+  uint8_t* T = (uint8_t*)scratch + 4096;
+  ck(cudaMemsetAsync(counters, 0, 4096, stream), "memset counters");
+  for (int k = 0; k < P.num_keys; ++k)
+    if (out_keys[k].mask && max_groups > 0)
+      ck(cudaMemsetAsync(out_keys[k].mask, 0, (size_t)((max_groups + 31) / 32) * 4, stream), "memset mask");
+  for (int j = 0; j < P.num_outs; ++j)
+    if (out_results[j].mask && max_groups > 0)
+      ck(cudaMemsetAsync(out_results[j].mask, 0, (size_t)((max_groups + 31) / 32) * 4, stream), "memset mask");
+  uint32_t host[4 + kMaxKeyCols + kMaxOutputs];
+  std::memset(host, 0, sizeof(host));
+  if (n > 0) {
+    DevInfo dev = dev_info();
+    SlotTemplate tmpl;
+    build_template(P, tmpl);
+    k_init_slots<<<dev.sms * 4, 256, 0, stream>>>(T, (int64_t)cap + 1, P.slot_bytes, tmpl);
+    TableRef G{T, cap - 1, P.slot_bytes, P.key_words, counters};
+    int grid = grid_for((const void*)k_aggregate<false>, 512, 0, 0);
+    grid = (int)std::min<int64_t>(grid, (n + 511) / 512);
+    k_aggregate<false><<<grid, 512, 0, stream>>>(P, G, 1, 0, tmpl);
+    k_finish_count<<<1, 1, 0, stream>>>(P, G);
+    ck(cudaGetLastError(), "aggregate launch");
+    ck(cudaMemcpyAsync(host, counters, 8, cudaMemcpyDeviceToHost, stream), "count d2h");
+    ck(cudaStreamSynchronize(stream), "aggregate sync");
+    if (host[1]) throw Error(ERR_LOGIC, "more groups than max_groups (table full)");
+    if ((int64_t)host[0] > max_groups)
+      throw Error(ERR_LOGIC, "more groups (" + std::to_string(host[0]) + ") than max_groups (" +
+                                 std::to_string(max_groups) + ")");
+    const int64_t G_n = host[0];
+    if (P.need_second_pass) {
+      int g2 = grid_for((const void*)k_var_pass, 256, 0, 0);
+      k_var_pass<<<g2, 256, 0, stream>>>(P, G);
+    }
+    OutPtrs O;
+    std::memset(&O, 0, sizeof(O));
+    for (int k = 0; k < P.num_keys; ++k) {
+      O.key_data[k] = out_keys[k].data;
+      O.key_mask[k] = out_keys[k].mask;
+    }
+    for (int j = 0; j < P.num_outs; ++j) {
+      O.out_data[j] = out_results[j].data;
+      O.out_mask[j] = out_results[j].mask;
+    }
+    O.counters = counters;
+    ck(cudaMemsetAsync(counters, 0, 512, stream), "memset");
+    if (G_n > 0) {
+      int64_t nslots = (int64_t)cap + 1;
+      int g3 = (int)std::min<int64_t>((nslots + 255) / 256, (int64_t)dev.sms * 8);
+      k_compact<<<g3, 256, 0, stream>>>(P, T, nslots, P.slot_bytes, G_n, 0, O);
+    }
+    ck(cudaGetLastError(), "compact launch");
+    ck(cudaMemcpyAsync(host, counters, 4 * (4 + P.num_keys + P.num_outs), cudaMemcpyDeviceToHost, stream),
+       "null counts d2h");
+    ck(cudaStreamSynchronize(stream), "compact sync");
+    if (host[1]) throw Error(ERR_CUDA, "internal error: compaction found more groups than were counted");
+    host[0] = (uint32_t)G_n;
+  } else {
+    ck(cudaStreamSynchronize(stream), "sync");
+  }
+  const int64_t groups = n > 0 ? (int64_t)host[0] : 0;
+  for (int k = 0; k < P.num_keys; ++k) {
+    out_keys[k].size = groups;
+    out_keys[k].null_count = n > 0 ? host[4 + k] : 0;
+  }
+  for (int j = 0; j < P.num_outs; ++j) {
+    out_results[j].size = groups;
+    out_results[j].null_count = n > 0 ? host[4 + P.num_keys + j] : 0;
+  }
+  return groups;
+}
+
+}  // namespace gb

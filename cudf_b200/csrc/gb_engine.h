@@ -100,6 +100,16 @@ void build_plan(const std::vector<Column>& keys, int null_policy, const std::vec
 Result aggregate(const std::vector<Column>& keys, int null_policy, const std::vector<Request>& reqs,
                  cudaStream_t stream, const Allocator& alloc, const Options& opt, Stats* stats);
 
+// Global-table aggregation with its table in caller-provided device scratch
+// and its results in caller-provided columns; makes no device allocation.
+int64_t aggregate_into_scratch(const std::vector<Column>& keys, int null_policy,
+                               const std::vector<Request>& reqs, cudaStream_t stream, void* scratch,
+                               size_t scratch_bytes, int64_t max_groups,
+                               std::vector<OutColumn>& out_keys, std::vector<OutColumn>& out_results);
+
+// Sets the message gb_last_error() returns on this thread.
+void set_last_error(const std::string& msg);
+
 // type helpers
 int type_width(int type_id);
 bool valid_agg(int type_id, int kind);

@@ -156,6 +156,33 @@ typedef struct gb_stats {
 GB_API int gb_set_tuning(gb_handle* handle, const gb_tuning* tuning);
 GB_API int gb_get_stats(const gb_handle* handle, gb_stats* out);
 
+/* Allocation-free groupby.  No counterpart in libcudf: its groupby always
+ * allocates its hash table and results through `mr`.  This entry point is for
+ * callers that cannot allocate device memory where they run -- code whose GPU
+ * memory belongs to another allocator that forbids outside allocations (a
+ * JVM or framework pool sized to the whole device), or loops where
+ * cudaMalloc/cudaFree are off limits because they synchronise the device.
+ * It runs the global-hash-table aggregation with its table in a fixed,
+ * file-scope device array of GB_NOALLOC_SCRATCH_BYTES (held by every GPU that
+ * loads the library until the process exits) and writes into caller-allocated
+ * outputs: it calls no cudaMalloc, cudaFree or other allocating routine.
+ *  - out_keys[num_keys] and out_results[sum of num_aggs] (request order): the
+ *    caller sets `data` (room for max_groups rows of the result type, see
+ *    gb_target_type) and, for nullable outputs, `null_mask` (room for
+ *    ceil(max_groups/32) words); the call fills type_id, size and null_count.
+ *  - the table needs (next_pow2(2*max_groups)+1) slots of the plan's slot size
+ *    plus 4 KiB of counters; larger requests are rejected with GB_ERR_LOGIC,
+ *    and so is a groupby that finds more than max_groups groups.
+ *  - the first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress); make that call before any stream capture.
+ *  - all calls share the array: calls that overlap on the GPU race and must be
+ *    serialised by the caller. */
+#define GB_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+GB_API int gb_aggregate_noalloc(const gb_column* keys, int32_t num_keys, int32_t null_policy,
+                                const gb_request* requests, int32_t num_requests, int64_t max_groups,
+                                gb_out_column* out_keys, gb_out_column* out_results,
+                                int64_t* num_groups, void* stream);
+
 /* Library version string. */
 GB_API const char* gb_version(void);
 
