@@ -4,9 +4,10 @@ path.  The compute path is the CUDA library built by ``cudf_b200.build``; there
 is no CPU fallback."""
 from . import aggregation
 from .column import Column, Table
+from .batch import BatchGroupBy
 from .groupby import GroupBy, GroupByRequest
 from .types import Kind, NullPolicy, Sorted, TypeId
 
-__all__ = ["aggregation", "Column", "Table", "GroupBy", "GroupByRequest", "Kind", "NullPolicy",
+__all__ = ["aggregation", "BatchGroupBy", "Column", "Table", "GroupBy", "GroupByRequest", "Kind", "NullPolicy",
            "Sorted", "TypeId"]
 __version__ = "0.1.0"

@@ -55,6 +55,12 @@ class GbStats(ctypes.Structure):
                 ("scatter_ms", ctypes.c_double)]
 
 
+class GbBatchStats(ctypes.Structure):
+    _fields_ = [("instances", ctypes.c_int64), ("tiles", ctypes.c_int64), ("smem_instances", ctypes.c_int64),
+                ("table_bytes", ctypes.c_int64), ("output_bytes", ctypes.c_int64),
+                ("kernels_per_run", ctypes.c_int32)]
+
+
 class GroupbyError(RuntimeError):
     """A failure reported by the engine; ``code`` is the GB_ERR_* value."""
 
@@ -88,6 +94,14 @@ SIGNATURES = {
     "gb_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GbTuning)]),
     "gb_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GbStats)]),
     "gb_version": (ctypes.c_char_p, []),
+    "gb_batch_prepare": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(GbColumn), ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.POINTER(GbRequest), ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "gb_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "gb_batch_result": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64),
+                                       ctypes.POINTER(GbOutColumn), ctypes.POINTER(GbOutColumn)]),
+    "gb_batch_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GbBatchStats)]),
+    "gb_batch_destroy": (None, [ctypes.c_void_p]),
     "gb_aggregate_noalloc": (ctypes.c_int, [ctypes.POINTER(GbColumn), ctypes.c_int32, ctypes.c_int32,
                                             ctypes.POINTER(GbRequest), ctypes.c_int32, ctypes.c_int64,
                                             ctypes.POINTER(GbOutColumn), ctypes.POINTER(GbOutColumn),

@@ -32,7 +32,7 @@ struct TableRef {
   unsigned int* counters;  // [0] groups, [1] overflow flag
 };
 
-__global__ void k_init_slots(uint8_t* T, int64_t nslots, int stride, const __grid_constant__ SlotTemplate tmpl)
+static __global__ void k_init_slots(uint8_t* T, int64_t nslots, int stride, const __grid_constant__ SlotTemplate tmpl)
 {
   int nw = stride / 8;
   int64_t total = nslots * nw;
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(512) k_aggregate(const __grid_constant__ Plan 
 
 // VARIANCE/STD second pass (cpp/src/groupby/hash/multi_pass_kernels.cuh:79-94):
 // per valid value, (x - mean)^2 / (n - ddof) added to the group's M2.
-__global__ void __launch_bounds__(256) k_var_pass(const __grid_constant__ Plan P, TableRef G)
+static __global__ void __launch_bounds__(256) k_var_pass(const __grid_constant__ Plan P, TableRef G)
 {
   const int64_t n = P.num_rows;
   for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n;
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(256) k_var_pass(const __grid_constant__ Plan P
   }
 }
 
-__global__ void k_finish_count(const __grid_constant__ Plan P, TableRef G)
+static __global__ void k_finish_count(const __grid_constant__ Plan P, TableRef G)
 {
   const uint8_t* special = G.T + (int64_t)(G.cap_mask + 1) * G.stride;
   if (*(const uint32_t*)(special + P.rows_off) > 0) atomicAdd(G.counters, 1u);
@@ -318,59 +318,70 @@ __device__ __forceinline__ uint64_t finalize(const Plan& P, const OutSpec& o, co
   }
 }
 
-__global__ void __launch_bounds__(256) k_compact(const __grid_constant__ Plan P, const uint8_t* T,
-                                                 int64_t nslots, int stride, int64_t limit, int dense,
-                                                 const __grid_constant__ OutPtrs O)
+// Writes the occupied slots among [base, base + blockDim.x) of one table into
+// dense output columns (positions reserved per block on O.counters[2]).
+// Every thread of the block calls it (it synchronises the block).
+__device__ __forceinline__ void compact_block(const Plan& P, const uint8_t* T, int64_t nslots, int stride,
+                                              int64_t limit, int dense, const OutPtrs& O, int64_t base,
+                                              void* scan_storage, unsigned int* s_base)
+{
+  using Scan = cub::BlockScan<int, 256>;
+  typename Scan::TempStorage& tmp = *(typename Scan::TempStorage*)scan_storage;
+  int64_t i = base + threadIdx.x;
+  const uint8_t* slot = T + i * (int64_t)stride;
+  bool occ = i < nslots && (dense || slot_occupied(P, slot, i == nslots - 1));
+  int local, total;
+  Scan(tmp).ExclusiveSum(occ ? 1 : 0, local, total);
+  if (threadIdx.x == 0) *s_base = total ? atomicAdd(O.counters + 2, (unsigned)total) : 0;
+  __syncthreads();
+  if (occ && (int64_t)*s_base + local >= limit) {
+    atomicOr(O.counters + 1, 1u);  // more occupied slots than counted groups
+    occ = false;
+  }
+  if (occ) {
+    int64_t pos = (int64_t)*s_base + local;
+    uint64_t w[2] = {((const uint64_t*)slot)[0], P.key_words == 2 ? ((const uint64_t*)slot)[1] : 0};
+    for (int k = 0; k < P.num_keys; ++k) {
+      const KeyCol& c = P.keys[k];
+      bool is_null = c.has_null_bit && ((w[c.null_word] >> c.null_shift) & 1);
+      uint64_t bits = c.width == 8 ? w[c.word] : (w[c.word] >> c.shift) & ((1ull << (8 * c.width)) - 1);
+      store_width(O.key_data[k], pos, c.width, is_null ? 0 : bits);
+      if (O.key_mask[k] && !is_null) atomicOr(O.key_mask[k] + (pos >> 5), 1u << (pos & 31));
+    }
+    for (int j = 0; j < P.num_outs; ++j) {
+      const OutSpec& o = P.outs[j];
+      bool valid;
+      uint64_t bits = finalize(P, o, slot, valid);
+      store_width(O.out_data[j], pos, o.out_width, valid ? bits : 0);
+      if (O.out_mask[j] && valid) atomicOr(O.out_mask[j] + (pos >> 5), 1u << (pos & 31));
+    }
+  }
+  // null counts (warp-aggregated)
+  for (int k = 0; k < P.num_keys; ++k) {
+    const KeyCol& c = P.keys[k];
+    bool is_null = occ && c.has_null_bit &&
+                   (((P.key_words == 2 && c.null_word == 1 ? ((const uint64_t*)slot)[1] : ((const uint64_t*)slot)[0])
+                     >> c.null_shift) & 1);
+    count_nulls(is_null, O.counters + 4 + k);
+  }
+  for (int j = 0; j < P.num_outs; ++j) {
+    bool valid = true;
+    if (occ && P.outs[j].nullable) finalize(P, P.outs[j], slot, valid);
+    count_nulls(occ && !valid, O.counters + 4 + P.num_keys + j);
+  }
+  __syncthreads();
+}
+
+static __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ Plan P, const uint8_t* T,
+                                                        int64_t nslots, int stride, int64_t limit, int dense,
+                                                        const __grid_constant__ OutPtrs O)
 {
   using Scan = cub::BlockScan<int, 256>;
   __shared__ typename Scan::TempStorage tmp;
   __shared__ unsigned int s_base;
   const int64_t step = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < nslots; base += step) {
-    int64_t i = base + threadIdx.x;
-    const uint8_t* slot = T + i * (int64_t)stride;
-    bool occ = i < nslots && (dense || slot_occupied(P, slot, i == nslots - 1));
-    int local, total;
-    Scan(tmp).ExclusiveSum(occ ? 1 : 0, local, total);
-    if (threadIdx.x == 0) s_base = total ? atomicAdd(O.counters + 2, (unsigned)total) : 0;
-    __syncthreads();
-    if (occ && (int64_t)s_base + local >= limit) {
-      atomicOr(O.counters + 1, 1u);  // more occupied slots than counted groups
-      occ = false;
-    }
-    if (occ) {
-      int64_t pos = (int64_t)s_base + local;
-      uint64_t w[2] = {((const uint64_t*)slot)[0], P.key_words == 2 ? ((const uint64_t*)slot)[1] : 0};
-      for (int k = 0; k < P.num_keys; ++k) {
-        const KeyCol& c = P.keys[k];
-        bool is_null = c.has_null_bit && ((w[c.null_word] >> c.null_shift) & 1);
-        uint64_t bits = c.width == 8 ? w[c.word] : (w[c.word] >> c.shift) & ((1ull << (8 * c.width)) - 1);
-        store_width(O.key_data[k], pos, c.width, is_null ? 0 : bits);
-        if (O.key_mask[k] && !is_null) atomicOr(O.key_mask[k] + (pos >> 5), 1u << (pos & 31));
-      }
-      for (int j = 0; j < P.num_outs; ++j) {
-        const OutSpec& o = P.outs[j];
-        bool valid;
-        uint64_t bits = finalize(P, o, slot, valid);
-        store_width(O.out_data[j], pos, o.out_width, valid ? bits : 0);
-        if (O.out_mask[j] && valid) atomicOr(O.out_mask[j] + (pos >> 5), 1u << (pos & 31));
-      }
-    }
-    // null counts (warp-aggregated)
-    for (int k = 0; k < P.num_keys; ++k) {
-      const KeyCol& c = P.keys[k];
-      bool is_null = occ && c.has_null_bit &&
-                     (((P.key_words == 2 && c.null_word == 1 ? ((const uint64_t*)slot)[1] : ((const uint64_t*)slot)[0])
-                       >> c.null_shift) & 1);
-      count_nulls(is_null, O.counters + 4 + k);
-    }
-    for (int j = 0; j < P.num_outs; ++j) {
-      bool valid = true;
-      if (occ && P.outs[j].nullable) finalize(P, P.outs[j], slot, valid);
-      count_nulls(occ && !valid, O.counters + 4 + P.num_keys + j);
-    }
-    __syncthreads();
-  }
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < nslots; base += step)
+    compact_block(P, T, nslots, stride, limit, dense, O, base, &tmp, &s_base);
 }
 
 // ---- group-count estimate from a key sample ----
@@ -378,7 +389,7 @@ __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ Plan P,
 // Also counts sampled keys per hash bucket (top kBucketBits bits of the hash)
 // so the partitioned path can size its regions.
 constexpr int kBucketBits = 14;
-__global__ void __launch_bounds__(256) k_sample(const __grid_constant__ Plan P, TableRef S, int64_t nsamp,
+static __global__ void __launch_bounds__(256) k_sample(const __grid_constant__ Plan P, TableRef S, int64_t nsamp,
                                                 unsigned int* buckets)
 {
   const int64_t n = P.num_rows;
@@ -399,7 +410,7 @@ __global__ void __launch_bounds__(256) k_sample(const __grid_constant__ Plan P, 
 }
 
 // counters: [4] distinct, [5] seen once, [6] seen twice
-__global__ void __launch_bounds__(256) k_sample_stats(const __grid_constant__ Plan P, TableRef S)
+static __global__ void __launch_bounds__(256) k_sample_stats(const __grid_constant__ Plan P, TableRef S)
 {
   int64_t nslots = (int64_t)S.cap_mask + 2;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nslots;

@@ -183,6 +183,35 @@ GB_API int gb_aggregate_noalloc(const gb_column* keys, int32_t num_keys, int32_t
                                 gb_out_column* out_keys, gb_out_column* out_results,
                                 int64_t* num_groups, void* stream);
 
+/* Batched groupby: many independent groupbys with one schema (same key types,
+ * value types and aggregations) aggregated by one persistent launch over a work
+ * queue of row tiles, optionally captured once as a CUDA graph and replayed.
+ * No counterpart in libcudf, where each groupby is its own call.
+ *  keys:     [num_instances * num_keys] column views, instance-major
+ *  requests: [num_instances * num_requests], instance-major
+ * gb_batch_prepare samples every instance and sizes its table and outputs;
+ * the views must stay valid (same shapes) for every gb_batch_run.  Results of
+ * instance i (views into batch-owned buffers, valid until the next run or
+ * gb_batch_destroy) come from gb_batch_result: keys[num_keys] and results in
+ * request order.  VARIANCE/STD are not supported in a batch. */
+typedef struct gb_batch gb_batch;
+typedef struct gb_batch_stats {
+  int64_t instances;
+  int64_t tiles;
+  int64_t smem_instances;   /* instances that use the shared-memory stage */
+  int64_t table_bytes;
+  int64_t output_bytes;
+  int32_t kernels_per_run;
+} gb_batch_stats;
+GB_API int gb_batch_prepare(int32_t num_instances, const gb_column* keys, int32_t num_keys,
+                            int32_t null_policy, const gb_request* requests, int32_t num_requests,
+                            int32_t use_graph, void* stream, const gb_allocator* mr, gb_batch** out);
+GB_API int gb_batch_run(gb_batch* batch, void* stream);
+GB_API int gb_batch_result(gb_batch* batch, int32_t instance, int64_t* num_groups,
+                           gb_out_column* keys, gb_out_column* results);
+GB_API int gb_batch_get_stats(const gb_batch* batch, gb_batch_stats* out);
+GB_API void gb_batch_destroy(gb_batch* batch);
+
 /* Library version string. */
 GB_API const char* gb_version(void);
 
