@@ -58,7 +58,7 @@ class GbStats(ctypes.Structure):
 class GbBatchStats(ctypes.Structure):
     _fields_ = [("instances", ctypes.c_int64), ("tiles", ctypes.c_int64), ("smem_instances", ctypes.c_int64),
                 ("table_bytes", ctypes.c_int64), ("output_bytes", ctypes.c_int64),
-                ("kernels_per_run", ctypes.c_int32)]
+                ("kernels_per_run", ctypes.c_int32), ("regrown", ctypes.c_int64)]
 
 
 class GroupbyError(RuntimeError):

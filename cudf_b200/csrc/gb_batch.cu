@@ -341,6 +341,88 @@ struct Batch::Impl {
   int sms = 148;
   BatchStats stats;
 
+
+  std::vector<int> key_types;
+  std::vector<bool> key_nullable;
+
+  // Tables, outputs, descriptors and compaction chunks for the current caps.
+  void layout(cudaStream_t stream)
+  {
+    const int stride = P.slot_bytes;
+    int64_t ts = 0;
+    std::vector<int64_t> tbase(ninst);
+    for (int i = 0; i < ninst; ++i) {
+      tbase[i] = ts;
+      ts += caps[i] + 1;
+    }
+    total_slots = ts;
+    d_tables.get(A, (size_t)ts * stride, stream);
+    for (int i = 0; i < ninst; ++i) {
+      insts[i].table = (uint8_t*)d_tables.p + (size_t)tbase[i] * stride;
+      insts[i].cap_mask = (uint64_t)caps[i] - 1;
+      insts[i].counters = (unsigned int*)d_counters.p + (size_t)i * counter_words;
+    }
+    ck(cudaMemcpyAsync(d_insts.p, insts.data(), sizeof(BatchInst) * ninst, cudaMemcpyHostToDevice, stream), "h2d");
+    // outputs, sized by table capacity (an upper bound on the group count):
+    // all data arrays first, then all masks in one region
+    size_t total = 0, mtotal = 0;
+    auto take = [](size_t& t, size_t bytes) {
+      size_t o = t;
+      t += (bytes + 255) & ~(size_t)255;
+      return o;
+    };
+    out_off.assign(ninst, {});
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int i = 0; i < ninst; ++i) {
+        int64_t rows = caps[i] + 1;
+        size_t mw = (size_t)((rows + 31) / 32) * 4;
+        int c = 0;
+        for (int k = 0; k < P.num_keys + nout; ++k, ++c) {
+          bool is_key = k < P.num_keys;
+          int tid = is_key ? key_types[k] : out_types[k - P.num_keys];
+          bool nullable = is_key ? (bool)key_nullable[k] : P.outs[k - P.num_keys].nullable != 0;
+          if (pass == 0) out_off[i].push_back({take(total, (size_t)rows * type_width(tid)), (size_t)-1});
+          else if (nullable) out_off[i][c].second = take(mtotal, mw);
+        }
+      }
+    }
+    mask_begin = total;
+    mask_end = total + mtotal;
+    for (int i = 0; i < ninst; ++i)
+      for (auto& oo : out_off[i])
+        if (oo.second != (size_t)-1) oo.second += total;
+    total += mtotal;
+    d_outputs.get(A, total, stream);
+    outs.assign(ninst, OutPtrs{});
+    for (int i = 0; i < ninst; ++i) {
+      OutPtrs& O = outs[i];
+      std::memset(&O, 0, sizeof(O));
+      uint8_t* base = (uint8_t*)d_outputs.p;
+      int c = 0;
+      for (int k = 0; k < P.num_keys; ++k, ++c) {
+        O.key_data[k] = base + out_off[i][c].first;
+        O.key_mask[k] = out_off[i][c].second == (size_t)-1 ? nullptr : (uint32_t*)(base + out_off[i][c].second);
+      }
+      for (int j = 0; j < nout; ++j, ++c) {
+        O.out_data[j] = base + out_off[i][c].first;
+        O.out_mask[j] = out_off[i][c].second == (size_t)-1 ? nullptr : (uint32_t*)(base + out_off[i][c].second);
+      }
+      O.counters = insts[i].counters;
+    }
+    d_outs.get(A, sizeof(OutPtrs) * ninst, stream);
+    ck(cudaMemcpyAsync(d_outs.p, outs.data(), sizeof(OutPtrs) * ninst, cudaMemcpyHostToDevice, stream), "h2d");
+    chunks.clear();
+    for (int i = 0; i < ninst; ++i)
+      for (int64_t b = 0; b < caps[i] + 1; b += 256) chunks.push_back(BatchChunk{i, 0, b});
+    d_chunks.get(A, sizeof(BatchChunk) * std::max<size_t>(1, chunks.size()), stream);
+    if (!chunks.empty())
+      ck(cudaMemcpyAsync(d_chunks.p, chunks.data(), sizeof(BatchChunk) * chunks.size(), cudaMemcpyHostToDevice, stream),
+         "h2d");
+    stats.table_bytes = (int64_t)ts * stride;
+    stats.output_bytes = (int64_t)total;
+    stats.kernels_per_run = 4 + (chunks.empty() ? 0 : 1);
+  }
+
   ~Impl()
   {
     if (exec) cudaGraphExecDestroy(exec);
@@ -463,16 +545,16 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
     if (scap_max * stride > budget) scap_max = 0;
   }
   B.caps.resize(ninst);
-  int64_t total_slots = 0;
-  std::vector<int64_t> tbase(ninst);
   for (int i = 0; i < ninst; ++i) {
     const int64_t n = B.insts[i].n_rows;
-    double d = st[i * 4 + 0], f1 = st[i * 4 + 1], f2 = st[i * 4 + 2], m = st[i * 4 + 3];
+    double d = st[i * 4 + 0], f1 = st[i * 4 + 1], m = st[i * 4 + 3];
     double est;
     if (n <= kSampleRows) est = std::max(1.0, d);
     else {
-      est = d + f1 * (f1 - 1) / (2 * (f2 + 1));
-      if (m > 0 && f1 > 0.9 * m) est = std::max(est, d * (double)n / m);
+      // Guaranteed-Error Estimator (Charikar et al. 2000): sqrt(n/m)*f1 + the keys
+      // seen more than once; within a factor sqrt(n/m) of the truth.  The
+      // trial run below grows any table that still overflows.
+      est = std::sqrt((double)n / std::max(1.0, m)) * f1 + (d - f1);
       est = std::min<double>((double)n, std::max(d, est));
     }
     est *= bo.growth;
@@ -480,8 +562,6 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
     cap = std::min<uint64_t>(cap, pow2_at_least((uint64_t)(2 * n + 2)));
     cap = std::max<uint64_t>(cap, 64);
     B.caps[i] = (int64_t)cap;
-    tbase[i] = total_slots;
-    total_slots += (int64_t)cap + 1;
     // shared-memory stage only when the instance's groups fit a tile's table
     int sc = 0;
     if (scap_max >= 64 && est * 2 <= scap_max && n > 4096) {
@@ -493,16 +573,8 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
     B.stats.est_groups_total += (int64_t)est;
     if (sc) ++B.stats.smem_instances;
   }
-  B.total_slots = total_slots;
-  B.d_tables.get(A, (size_t)total_slots * stride, stream);
   B.d_counters.get(A, (size_t)ninst * B.counter_words * 4, stream);
   B.d_work.get(A, 16, stream);
-  for (int i = 0; i < ninst; ++i) {
-    B.insts[i].table = (uint8_t*)B.d_tables.p + (size_t)tbase[i] * stride;
-    B.insts[i].cap_mask = (uint64_t)B.caps[i] - 1;
-    B.insts[i].counters = (unsigned int*)B.d_counters.p + (size_t)i * B.counter_words;
-  }
-  ck(cudaMemcpyAsync(B.d_insts.p, B.insts.data(), sizeof(BatchInst) * ninst, cudaMemcpyHostToDevice, stream), "h2d");
   // tiles: instances cut into kBatchTile-row pieces, largest first
   std::vector<int> order(ninst);
   for (int i = 0; i < ninst; ++i) order[i] = i;
@@ -515,62 +587,6 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
   if (!B.tiles.empty())
     ck(cudaMemcpyAsync(B.d_tiles.p, B.tiles.data(), sizeof(BatchTile) * B.tiles.size(), cudaMemcpyHostToDevice, stream),
        "h2d");
-  // outputs, sized by table capacity (an upper bound on the group count):
-  // all data arrays first, then all masks in one region
-  size_t total = 0, mtotal = 0;
-  auto take = [](size_t& t, size_t bytes) {
-    size_t o = t;
-    t += (bytes + 255) & ~(size_t)255;
-    return o;
-  };
-  B.out_off.assign(ninst, {});
-  for (int pass = 0; pass < 2; ++pass) {
-    for (int i = 0; i < ninst; ++i) {
-      int64_t rows = B.caps[i] + 1;
-      size_t mw = (size_t)((rows + 31) / 32) * 4;
-      int c = 0;
-      for (int k = 0; k < B.P.num_keys + B.nout; ++k, ++c) {
-        bool is_key = k < B.P.num_keys;
-        int tid = is_key ? keys[i][k].type_id : B.out_types[k - B.P.num_keys];
-        bool nullable = is_key ? k0[k].mask != nullptr : B.P.outs[k - B.P.num_keys].nullable != 0;
-        if (pass == 0) B.out_off[i].push_back({take(total, (size_t)rows * type_width(tid)), (size_t)-1});
-        else if (nullable) B.out_off[i][c].second = take(mtotal, mw);
-      }
-    }
-  }
-  B.mask_begin = total;
-  B.mask_end = total + mtotal;
-  for (int i = 0; i < ninst; ++i)
-    for (auto& oo : B.out_off[i])
-      if (oo.second != (size_t)-1) oo.second += total;
-  total += mtotal;
-  B.d_outputs.get(A, total, stream);
-  B.outs.assign(ninst, OutPtrs{});
-  for (int i = 0; i < ninst; ++i) {
-    OutPtrs& O = B.outs[i];
-    std::memset(&O, 0, sizeof(O));
-    uint8_t* base = (uint8_t*)B.d_outputs.p;
-    int c = 0;
-    for (int k = 0; k < B.P.num_keys; ++k, ++c) {
-      O.key_data[k] = base + B.out_off[i][c].first;
-      O.key_mask[k] = B.out_off[i][c].second == (size_t)-1 ? nullptr : (uint32_t*)(base + B.out_off[i][c].second);
-    }
-    for (int j = 0; j < B.nout; ++j, ++c) {
-      O.out_data[j] = base + B.out_off[i][c].first;
-      O.out_mask[j] = B.out_off[i][c].second == (size_t)-1 ? nullptr : (uint32_t*)(base + B.out_off[i][c].second);
-    }
-    O.counters = B.insts[i].counters;
-  }
-  B.d_outs.get(A, sizeof(OutPtrs) * ninst, stream);
-  ck(cudaMemcpyAsync(B.d_outs.p, B.outs.data(), sizeof(OutPtrs) * ninst, cudaMemcpyHostToDevice, stream), "h2d");
-  B.chunks.clear();
-  for (int i = 0; i < ninst; ++i)
-    for (int64_t b = 0; b < B.caps[i] + 1; b += 256) B.chunks.push_back(BatchChunk{i, 0, b});
-  B.d_chunks.get(A, sizeof(BatchChunk) * std::max<size_t>(1, B.chunks.size()), stream);
-  if (!B.chunks.empty())
-    ck(cudaMemcpyAsync(B.d_chunks.p, B.chunks.data(), sizeof(BatchChunk) * B.chunks.size(), cudaMemcpyHostToDevice,
-                       stream),
-       "h2d");
   if (!B.h_counters) ck(cudaMallocHost((void**)&B.h_counters, (size_t)ninst * B.counter_words * 4), "cudaMallocHost");
   // launch shapes
   B.smem_bytes = scap_max * stride;
@@ -581,9 +597,24 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
   B.grid_compact = sms * 8;
   B.stats.instances = ninst;
   B.stats.tiles = (int64_t)B.tiles.size();
-  B.stats.table_bytes = (int64_t)total_slots * stride;
-  B.stats.output_bytes = (int64_t)total;
-  B.stats.kernels_per_run = 4 + (B.chunks.empty() ? 0 : 1);
+  B.key_types.clear();
+  for (auto& k : keys[0]) B.key_types.push_back(k.type_id);
+  B.key_nullable.clear();
+  for (auto& k : k0) B.key_nullable.push_back(k.mask != nullptr);
+  B.layout(stream);
+  // trial runs: grow the tables (and outputs) of instances that overflowed
+  for (int round = 0;; ++round) {
+    B.enqueue(stream);
+    ck(cudaStreamSynchronize(stream), "trial sync");
+    std::vector<int> over;
+    for (int i = 0; i < ninst; ++i)
+      if (B.h_counters[(size_t)i * B.counter_words + 1]) over.push_back(i);
+    if (over.empty()) break;
+    if (round >= 6) throw Error(ERR_CUDA, "batch tables keep overflowing");
+    B.stats.regrown += (int64_t)over.size();
+    for (int i : over) B.caps[i] *= 4;
+    B.layout(stream);
+  }
   if (bo.use_graph) {
     cudaStream_t cs;
     ck(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
@@ -761,6 +792,7 @@ int gb_batch_get_stats(const gb_batch* b, gb_batch_stats* out)
     out->table_bytes = s.table_bytes;
     out->output_bytes = s.output_bytes;
     out->kernels_per_run = s.kernels_per_run;
+    out->regrown = s.regrown;
   });
 }
 

@@ -21,6 +21,7 @@ struct BatchStats {
   int64_t table_bytes = 0;
   int64_t output_bytes = 0;
   int64_t overflowed = 0;
+  int64_t regrown = 0;  // instance tables grown after a trial run overflowed
   int kernels_per_run = 0;
 };
 

@@ -202,6 +202,7 @@ typedef struct gb_batch_stats {
   int64_t table_bytes;
   int64_t output_bytes;
   int32_t kernels_per_run;
+  int64_t regrown;          /* instance tables grown after a trial run overflowed */
 } gb_batch_stats;
 GB_API int gb_batch_prepare(int32_t num_instances, const gb_column* keys, int32_t num_keys,
                             int32_t null_policy, const gb_request* requests, int32_t num_requests,
