@@ -6,8 +6,9 @@ from . import aggregation
 from .column import Column, Table
 from .batch import BatchGroupBy
 from .groupby import GroupBy, GroupByRequest
+from .serving import Server
 from .types import Kind, NullPolicy, Sorted, TypeId
 
 __all__ = ["aggregation", "BatchGroupBy", "Column", "Table", "GroupBy", "GroupByRequest", "Kind", "NullPolicy",
-           "Sorted", "TypeId"]
+           "Server", "Sorted", "TypeId"]
 __version__ = "0.1.0"

@@ -61,6 +61,22 @@ class GbBatchStats(ctypes.Structure):
                 ("kernels_per_run", ctypes.c_int32), ("regrown", ctypes.c_int64)]
 
 
+class GbServerOptions(ctypes.Structure):
+    _fields_ = [("memory_cap_bytes", ctypes.c_int64), ("max_batch_queries", ctypes.c_int32),
+                ("max_batch_rows", ctypes.c_int64), ("workers", ctypes.c_int32)]
+
+
+class GbQueryInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("latency_s", ctypes.c_double), ("queue_s", ctypes.c_double),
+                ("num_groups", ctypes.c_int64)]
+
+
+class GbServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("batches", ctypes.c_int64),
+                ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double), ("queries_per_s", ctypes.c_double),
+                ("peak_admitted_bytes", ctypes.c_int64)]
+
+
 class GroupbyError(RuntimeError):
     """A failure reported by the engine; ``code`` is the GB_ERR_* value."""
 
@@ -102,6 +118,15 @@ SIGNATURES = {
                                        ctypes.POINTER(GbOutColumn), ctypes.POINTER(GbOutColumn)]),
     "gb_batch_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GbBatchStats)]),
     "gb_batch_destroy": (None, [ctypes.c_void_p]),
+    "gb_server_create": (ctypes.c_int, [ctypes.POINTER(GbServerOptions), ctypes.POINTER(ctypes.c_void_p)]),
+    "gb_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GbColumn), ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.POINTER(GbRequest), ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]),
+    "gb_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(GbQueryInfo)]),
+    "gb_server_result": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
+                                        ctypes.POINTER(GbOutColumn), ctypes.POINTER(GbOutColumn)]),
+    "gb_server_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    "gb_server_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GbServerStats)]),
+    "gb_server_destroy": (None, [ctypes.c_void_p]),
     "gb_aggregate_noalloc": (ctypes.c_int, [ctypes.POINTER(GbColumn), ctypes.c_int32, ctypes.c_int32,
                                             ctypes.POINTER(GbRequest), ctypes.c_int32, ctypes.c_int64,
                                             ctypes.POINTER(GbOutColumn), ctypes.POINTER(GbOutColumn),

@@ -450,6 +450,56 @@ struct Batch::Impl {
   }
 };
 
+std::vector<int64_t> batch_estimate_groups(const std::vector<std::vector<Column>>& keys, int null_policy,
+                                           const std::vector<std::vector<Request>>&, cudaStream_t stream,
+                                           const Allocator& A)
+{
+  const int ninst = (int)keys.size();
+  std::vector<int64_t> out(ninst, 1);
+  if (ninst == 0) return out;
+  std::vector<Column> k0 = keys[0];
+  static const uint32_t kAnyMask = 0;
+  for (int i = 0; i < ninst; ++i) {
+    if (keys[i].size() != k0.size()) throw Error(ERR_LOGIC, "key layouts differ");
+    for (size_t k = 0; k < k0.size(); ++k) {
+      if (keys[i][k].type_id != k0[k].type_id) throw Error(ERR_LOGIC, "key types differ");
+      if (keys[i][k].mask) k0[k].mask = &kAnyMask;
+    }
+  }
+  Plan P;
+  std::vector<int> ot;
+  build_plan(k0, null_policy, {}, P, ot);
+  std::vector<BatchInst> insts(ninst);
+  for (int i = 0; i < ninst; ++i) {
+    std::memset(&insts[i], 0, sizeof(BatchInst));
+    for (size_t k = 0; k < keys[i].size(); ++k) {
+      insts[i].key_data[k] = keys[i][k].data;
+      insts[i].key_mask[k] = keys[i][k].mask;
+      insts[i].key_off[k] = keys[i][k].offset;
+    }
+    insts[i].n_rows = keys[i][0].size;
+  }
+  DevBuf d_insts, d_stats;
+  d_insts.get(A, sizeof(BatchInst) * ninst, stream);
+  d_stats.get(A, (size_t)ninst * 16, stream);
+  ck(cudaMemcpyAsync(d_insts.p, insts.data(), sizeof(BatchInst) * ninst, cudaMemcpyHostToDevice, stream), "h2d");
+  size_t sm = (size_t)kSampleSlots * 32;
+  ck(cudaFuncSetAttribute(k_batch_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), "attr");
+  k_batch_sample<<<ninst, 256, sm, stream>>>(P, (const BatchInst*)d_insts.p, (unsigned int*)d_stats.p);
+  ck(cudaGetLastError(), "sketch launch");
+  std::vector<unsigned int> st((size_t)ninst * 4);
+  ck(cudaMemcpyAsync(st.data(), d_stats.p, st.size() * 4, cudaMemcpyDeviceToHost, stream), "d2h");
+  ck(cudaStreamSynchronize(stream), "sketch sync");
+  for (int i = 0; i < ninst; ++i) {
+    const int64_t n = insts[i].n_rows;
+    double d = st[i * 4 + 0], f1 = st[i * 4 + 1], m = st[i * 4 + 3];
+    double est = n <= kSampleRows ? std::max(1.0, d)
+                                  : std::min<double>((double)n, std::max(d, std::sqrt((double)n / std::max(1.0, m)) * f1 + (d - f1)));
+    out[i] = (int64_t)std::max(1.0, est);
+  }
+  return out;
+}
+
 Batch::Batch() : impl(new Impl) {}
 Batch::~Batch() = default;
 

@@ -25,6 +25,12 @@ struct BatchStats {
   int kernels_per_run = 0;
 };
 
+// Device-side key sketch: estimated group count of each instance (one
+// sampling launch; every instance must share the key layout).
+std::vector<int64_t> batch_estimate_groups(const std::vector<std::vector<Column>>& keys, int null_policy,
+                                           const std::vector<std::vector<Request>>& reqs, cudaStream_t stream,
+                                           const Allocator& A);
+
 class Batch {
  public:
   Batch();

@@ -213,6 +213,48 @@ GB_API int gb_batch_result(gb_batch* batch, int32_t instance, int64_t* num_group
 GB_API int gb_batch_get_stats(const gb_batch* batch, gb_batch_stats* out);
 GB_API void gb_batch_destroy(gb_batch* batch);
 
+/* Serving loop: continuous batching of groupby queries (no counterpart in
+ * libcudf).  gb_server_submit enqueues a query whose columns are resident on
+ * the device (they must stay valid until the query is released).  A
+ * dispatcher thread admits queries in arrival order while the estimated device
+ * memory (hash table + results, from the row count and a device-side key
+ * sketch) of all admitted, unreleased queries stays under memory_cap_bytes, and
+ * packs each round of admitted queries into one batched launch run by the next
+ * idle worker (each worker has its own stream, so batches overlap on the GPU).
+ * gb_server_wait blocks until a query completes; gb_server_result gives views
+ * of its results (valid until gb_server_release). */
+typedef struct gb_server gb_server;
+typedef struct gb_server_options {
+  int64_t memory_cap_bytes;   /* admission cap (default 150 GiB) */
+  int32_t max_batch_queries;  /* queries per batched launch (default 256) */
+  int64_t max_batch_rows;     /* rows per batched launch (default 400 Mi) */
+  int32_t workers;            /* worker threads / streams (default 2) */
+} gb_server_options;
+typedef struct gb_query_info {
+  int32_t status;             /* 2 done, 3 failed */
+  double latency_s;           /* arrival to completion */
+  double queue_s;             /* arrival to admission */
+  int64_t num_groups;
+} gb_query_info;
+typedef struct gb_server_stats {
+  int64_t completed;
+  int64_t failed;
+  int64_t batches;
+  double p50_s;
+  double p99_s;
+  double queries_per_s;       /* completed / (last completion - first arrival) */
+  int64_t peak_admitted_bytes;
+} gb_server_stats;
+GB_API int gb_server_create(const gb_server_options* opt, gb_server** out);
+GB_API int gb_server_submit(gb_server* server, const gb_column* keys, int32_t num_keys, int32_t null_policy,
+                            const gb_request* requests, int32_t num_requests, int64_t* query_id);
+GB_API int gb_server_wait(gb_server* server, int64_t query_id, double timeout_s, gb_query_info* info);
+GB_API int gb_server_result(gb_server* server, int64_t query_id, int64_t* num_groups,
+                            gb_out_column* keys, gb_out_column* results);
+GB_API int gb_server_release(gb_server* server, int64_t query_id);
+GB_API int gb_server_get_stats(gb_server* server, gb_server_stats* out);
+GB_API void gb_server_destroy(gb_server* server);
+
 /* Library version string. */
 GB_API const char* gb_version(void);
 
