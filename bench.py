@@ -412,6 +412,116 @@ def run_batch(args):
     return 0
 
 
+def run_serve(args):
+    """Serving stream: Poisson arrivals at --rate queries/s for --duration s;
+    each query a groupby over int64 keys (cardinality log-uniform [10, 1e6]),
+    rows log-uniform [1e4, 2e7], int64 and float64 values with 10% nulls,
+    sum/count/mean; admission capped at 150 GB; seed 4.  Queries read prefixes of
+    a pool of device-resident tables.  The batched server (continuous batching)
+    is compared with plain one-aggregate()-per-query serving in arrival order."""
+    import threading
+    import torch
+    import cudf_b200 as cb
+    from cudf_b200 import aggregation as agg
+    from cudf_b200.column import pack_mask
+    from cudf_b200.types import TypeId
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(4)
+    pool_n = 20_000_000
+    pool = []
+    g = torch.Generator(device=dev)
+    g.manual_seed(4)
+    cards = np.exp(np.linspace(np.log(10), np.log(1e6), args.pool)).astype(np.int64)
+    for c in cards.tolist():
+        k = torch.randint(0, int(c), (pool_n,), device=dev, generator=g, dtype=torch.int64) * 7919
+        v1 = torch.randint(-10**9, 10**9 + 1, (pool_n,), device=dev, generator=g, dtype=torch.int64)
+        v2 = torch.randn(pool_n, device=dev, generator=g, dtype=torch.float64)
+        m1 = pack_mask(torch.rand(pool_n, device=dev, generator=g) >= 0.1)
+        m2 = pack_mask(torch.rand(pool_n, device=dev, generator=g) >= 0.1)
+        pool.append((k, v1, v2, m1, m2))
+    torch.cuda.synchronize()
+    nq = int(rng.poisson(args.rate * args.duration))
+    arrivals = np.sort(rng.uniform(0, args.duration, nq))
+    which = rng.integers(0, args.pool, nq)
+    rows = np.exp(rng.uniform(np.log(1e4), np.log(2e7), nq)).astype(np.int64)
+
+    def query(i):
+        k, v1, v2, m1, m2 = pool[which[i]]
+        n = int(rows[i])
+        kt = cb.Table([cb.Column(TypeId.INT64, k, size=n)])
+        aggs = [agg.sum(), agg.count(), agg.mean()]
+        return kt, [cb.GroupByRequest(cb.Column(TypeId.INT64, v1, m1, size=n), aggs),
+                    cb.GroupByRequest(cb.Column(TypeId.FLOAT64, v2, m2, size=n), aggs)]
+
+    qs = [query(i) for i in range(nq)]
+    # plain single-query latency (no queueing): a sample of queries run alone
+    for i in range(5):
+        cb.GroupBy(qs[i][0]).aggregate(qs[i][1])
+    alone = []
+    for i in range(min(nq, 200)):
+        t = time.perf_counter()
+        cb.GroupBy(qs[i][0]).aggregate(qs[i][1])
+        alone.append(time.perf_counter() - t)
+    alone_p50 = float(np.median(alone))
+
+    def plain():
+        lat = []
+        t0 = time.perf_counter()
+        for i in range(nq):
+            now = time.perf_counter() - t0
+            if now < arrivals[i]:
+                time.sleep(arrivals[i] - now)
+            cb.GroupBy(qs[i][0]).aggregate(qs[i][1])
+            lat.append(time.perf_counter() - t0 - arrivals[i])
+        span = time.perf_counter() - t0
+        return {"queries_per_s": nq / span, "p50_s": float(np.percentile(lat, 50)),
+                "p99_s": float(np.percentile(lat, 99)), "completed": nq}
+
+    def batched():
+        srv = cb.Server(memory_cap_bytes=150 << 30, workers=args.workers)
+        ids = [None] * nq
+        done = threading.Event()
+
+        def collector():
+            for i in range(nq):
+                while ids[i] is None:
+                    time.sleep(1e-4)
+                srv.wait(ids[i], timeout_s=600)
+                srv.release(ids[i])
+            done.set()
+
+        th = threading.Thread(target=collector)
+        th.start()
+        t0 = time.perf_counter()
+        for i in range(nq):
+            now = time.perf_counter() - t0
+            if now < arrivals[i]:
+                time.sleep(arrivals[i] - now)
+            ids[i] = srv.submit(*qs[i])
+        th.join()
+        st = srv.stats()
+        srv.close()
+        return st
+
+    b = batched()
+    p = plain()
+    line = {"metric": f"served groupby queries/s (Poisson {args.rate}/s for {args.duration}s)",
+            "value": b["queries_per_s"], "unit": "queries/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64",
+            "data": "synthetic",
+            "config": {"workload": "serving stream: int64 keys (cardinality log-uniform [10,1e6]), rows "
+                                   "log-uniform [1e4,2e7], int64+f64 values 10% nulls, sum/count/mean, "
+                                   "admission cap 150 GB", "queries": nq, "rate": args.rate,
+                       "duration_s": args.duration, "pool_tables": args.pool, "workers": args.workers,
+                       "mean_rows": float(rows.mean())},
+            "batched": b, "plain": p, "plain_single_query_latency_s": alone_p50,
+            "qps_ratio_vs_plain": b["queries_per_s"] / p["queries_per_s"],
+            "p99_over_plain_single": b["p99_s"] / alone_p50}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -422,11 +532,17 @@ def main():
     ap.add_argument("--tuning", default="")
     ap.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE_ROWS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="single", choices=["single", "batch"])
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve"])
     ap.add_argument("--instances", type=int, default=4096)
+    ap.add_argument("--rate", type=float, default=2000.0)
+    ap.add_argument("--duration", type=float, default=5.0)
+    ap.add_argument("--pool", type=int, default=16)
+    ap.add_argument("--workers", type=int, default=2)
     args = ap.parse_args()
     if args.workload == "batch" and args.impl == "engine":
         return run_batch(args)
+    if args.workload == "serve" and args.impl == "engine":
+        return run_serve(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_engine(args)

@@ -12,7 +12,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -162,7 +165,14 @@ static __global__ void __launch_bounds__(kBatchThreads) k_batch_aggregate(const 
     __syncthreads();
     TableRef G{I.table, I.cap_mask, stride, sp.key_words, I.counters};
     const uint64_t smask = (uint64_t)(scap > 0 ? scap : 1) - 1;
-    for (int64_t row = tl.begin + threadIdx.x; row < tl.end; row += blockDim.x) {
+    // an instance whose table overflowed is re-run with a larger table: skip
+    const int64_t row_end = *(volatile unsigned int*)(I.counters + 1) ? tl.begin : tl.end;
+    int since_check = 0;
+    for (int64_t row = tl.begin + threadIdx.x; row < row_end; row += blockDim.x) {
+      if (++since_check == 64) {
+        since_check = 0;
+        if (*(volatile unsigned int*)(I.counters + 1)) break;
+      }
       uint64_t w0, w1;
       if (!pack_key(sp, row, w0, w1)) continue;
       uint64_t h = hash_key(w0, w1, sp.key_words);
@@ -573,6 +583,8 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   B.sms = sms;
 
+  auto tnow = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+  double t_begin = tnow();
   // ---- per-instance group-count estimates from one sample launch ----
   B.d_insts.get(A, sizeof(BatchInst) * ninst, stream);
   ck(cudaMemcpyAsync(B.d_insts.p, B.insts.data(), sizeof(BatchInst) * ninst, cudaMemcpyHostToDevice, stream), "h2d");
@@ -586,6 +598,7 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
     ck(cudaMemcpyAsync(st.data(), B.d_stats.p, st.size() * 4, cudaMemcpyDeviceToHost, stream), "d2h");
     ck(cudaStreamSynchronize(stream), "sample sync");
   }
+  B.stats.sample_s = tnow() - t_begin;
   // ---- sizing ----
   const int stride = B.P.slot_bytes;
   int scap_max = 1;
@@ -651,9 +664,13 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
   for (auto& k : keys[0]) B.key_types.push_back(k.type_id);
   B.key_nullable.clear();
   for (auto& k : k0) B.key_nullable.push_back(k.mask != nullptr);
+  double t_lay = tnow();
   B.layout(stream);
+  B.stats.layout_s = tnow() - t_lay;
   // trial runs: grow the tables (and outputs) of instances that overflowed
+  double t_trial = tnow();
   for (int round = 0;; ++round) {
+    B.stats.trial_rounds = round + 1;
     B.enqueue(stream);
     ck(cudaStreamSynchronize(stream), "trial sync");
     std::vector<int> over;
@@ -664,6 +681,14 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
     B.stats.regrown += (int64_t)over.size();
     for (int i : over) B.caps[i] *= 4;
     B.layout(stream);
+  }
+  B.stats.trial_s = tnow() - t_trial;
+  if (std::getenv("GB_TRACE")) {
+    int64_t rows = 0;
+    for (auto& I : B.insts) rows += I.n_rows;
+    std::fprintf(stderr, "[gb batch] %d inst %lld rows: sample %.3fs layout %.3fs trial %.3fs x%d tables %.2fGB out %.2fGB\n",
+                 ninst, (long long)rows, B.stats.sample_s, B.stats.layout_s, B.stats.trial_s, B.stats.trial_rounds,
+                 B.stats.table_bytes / 1e9, B.stats.output_bytes / 1e9);
   }
   if (bo.use_graph) {
     cudaStream_t cs;
@@ -688,9 +713,11 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
 void Batch::run(cudaStream_t stream)
 {
   Impl& B = *impl;
+  auto t0 = std::chrono::steady_clock::now();
   if (B.exec) ck(cudaGraphLaunch(B.exec, stream), "graph launch");
   else B.enqueue(stream);
   ck(cudaStreamSynchronize(stream), "batch sync");
+  B.stats.run_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   int over = 0;
   for (int i = 0; i < B.ninst; ++i) {
     const unsigned int* c = B.h_counters + (size_t)i * B.counter_words;

@@ -22,6 +22,8 @@ struct BatchStats {
   int64_t output_bytes = 0;
   int64_t overflowed = 0;
   int64_t regrown = 0;  // instance tables grown after a trial run overflowed
+  int trial_rounds = 0;
+  double sample_s = 0, layout_s = 0, trial_s = 0, run_s = 0;
   int kernels_per_run = 0;
 };
 

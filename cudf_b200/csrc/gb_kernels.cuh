@@ -16,6 +16,10 @@
 namespace gb {
 
 constexpr int kMaxSlotBytes = 1024;
+// Longest probe run of a global table.  At load <= 0.5 linear probing needs a
+// few probes; a run this long means the table is (nearly) full, which is
+// reported as overflow (the host regrows the table) instead of scanning it.
+constexpr uint64_t kMaxProbes = 4096;
 
 // Identity contents of an empty slot, as 8-byte words (slot strides are
 // multiples of 8; an odd multiple spreads a field of consecutive slots over
@@ -76,8 +80,8 @@ __device__ __forceinline__ int64_t global_slot(const Plan& P, const TableRef& G,
 {
   bool ins;
   int64_t i = P.key_words == 1
-                ? find_or_insert1(G.T, G.stride, G.cap_mask, w0, h, (int)min((uint64_t)INT32_MAX, G.cap_mask + 1), ins)
-                : find_or_insert2(G.T, G.stride, G.cap_mask, w0, w1, h, (int)min((uint64_t)INT32_MAX, G.cap_mask + 1), ins);
+                ? find_or_insert1(G.T, G.stride, G.cap_mask, w0, h, (int)min(kMaxProbes, G.cap_mask + 1), ins)
+                : find_or_insert2(G.T, G.stride, G.cap_mask, w0, w1, h, (int)min(kMaxProbes, G.cap_mask + 1), ins);
   if (ins) atomicAdd(s_new, 1u);
   return i;
 }
@@ -130,8 +134,14 @@ __global__ void __launch_bounds__(512) k_aggregate(const __grid_constant__ Plan 
   __syncthreads();
   const uint64_t smask = (uint64_t)scap - 1;
   const int64_t n = P.num_rows;
+  int since_check = 0;
   for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n;
        row += (int64_t)gridDim.x * blockDim.x) {
+    // once the table overflowed the host re-runs with a larger one: stop early
+    if (++since_check == 64) {
+      since_check = 0;
+      if (*(volatile unsigned int*)(G.counters + 1)) break;
+    }
     uint64_t w0, w1;
     if (!pack_key(P, row, w0, w1)) continue;
     uint64_t h = hash_key(w0, w1, P.key_words);

@@ -74,6 +74,8 @@ struct Server {
   std::vector<double> latencies;
   int64_t completed = 0, failed = 0, batches = 0;
   double first_arrive = -1, last_done = 0;
+  double sketch_s = 0, prepare_s = 0, run_s = 0, trial_s = 0;
+  int64_t trial_rounds = 0;
   cudaStream_t sketch_stream = nullptr;
 
   // device-side sketch of a set of queries: estimated groups per query, one
@@ -129,7 +131,9 @@ struct Server {
         // group arrivals by schema-compatible runs (same layout as the first)
         std::vector<double> est;
         try {
+          double t0 = now_s();
           est = sketch(arrivals);
+          sketch_s += now_s() - t0;
         } catch (const std::exception& ex) {
           est.assign(arrivals.size(), 0.0);
           for (auto& q : arrivals) q->est_bytes = -1, q->error = ex.what();
@@ -230,6 +234,13 @@ struct Server {
         double t_done = now_s();
         std::lock_guard<std::mutex> lk(mu);
         ++batches;
+        {
+          const BatchStats& bs = b->stats();
+          prepare_s += bs.sample_s + bs.layout_s + bs.trial_s;
+          trial_s += bs.trial_s;
+          run_s += bs.run_s;
+          trial_rounds += bs.trial_rounds;
+        }
         for (size_t i = 0; i < qs.size(); ++i) {
           auto& q = qs[i];
           q->launch = t_launch;
@@ -429,6 +440,10 @@ int gb_server_get_stats(gb_server* sv, gb_server_stats* out)
     double span = S.last_done - S.first_arrive;
     out->queries_per_s = span > 0 ? S.completed / span : 0;
     out->peak_admitted_bytes = S.peak_in_use;
+    out->sketch_s = S.sketch_s;
+    out->prepare_s = S.prepare_s;
+    out->run_s = S.run_s;
+    out->trial_rounds = S.trial_rounds;
   });
 }
 

@@ -244,6 +244,10 @@ typedef struct gb_server_stats {
   double p99_s;
   double queries_per_s;       /* completed / (last completion - first arrival) */
   int64_t peak_admitted_bytes;
+  double sketch_s;            /* dispatcher time in the key sketch */
+  double prepare_s;           /* workers' batch sizing time (sample, layout, trial runs) */
+  double run_s;               /* workers' batch run time */
+  int64_t trial_rounds;
 } gb_server_stats;
 GB_API int gb_server_create(const gb_server_options* opt, gb_server** out);
 GB_API int gb_server_submit(gb_server* server, const gb_column* keys, int32_t num_keys, int32_t null_policy,
