@@ -131,7 +131,9 @@ static __global__ void k_batch_init(uint8_t* T, int64_t nslots, int stride, cons
   }
 }
 
-// Persistent aggregation over the tile queue.
+// Aggregation of the tile list: one CTA per tile (largest instances first), so
+// that kernels of other streams (the serving loop's sketch) interleave at tile
+// granularity.
 static __global__ void __launch_bounds__(kBatchThreads) k_batch_aggregate(const __grid_constant__ Plan P,
                                                                           const BatchInst* insts,
                                                                           const BatchTile* tiles, int64_t ntiles,
@@ -139,21 +141,27 @@ static __global__ void __launch_bounds__(kBatchThreads) k_batch_aggregate(const 
                                                                           const __grid_constant__ SlotTemplate tmpl)
 {
   extern __shared__ __align__(16) uint8_t smem[];
-  __shared__ Plan sp;
-  __shared__ int64_t s_tile;
+  __shared__ __align__(16) Plan sp;
   __shared__ unsigned int s_new, s_used;
-  if (threadIdx.x == 0) sp = P;
-  const int stride = P.slot_bytes;
-  const int nw = stride / 8;
-  for (;;) {
+  {
+    const int4* src = (const int4*)&P;
+    int4* dst = (int4*)&sp;
+    for (int i = threadIdx.x; i < (int)(sizeof(Plan) / 16); i += blockDim.x) dst[i] = src[i];
     if (threadIdx.x == 0) {
-      s_tile = (int64_t)atomicAdd(work, 1u);
+      for (size_t b = (sizeof(Plan) / 16) * 16; b < sizeof(Plan); ++b) ((char*)&sp)[b] = ((const char*)&P)[b];
       s_new = 0;
       s_used = 0;
     }
+  }
+  (void)work;
+  const int stride = P.slot_bytes;
+  const int nw = stride / 8;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     __syncthreads();
-    const int64_t t = s_tile;
-    if (t >= ntiles) break;
+    if (threadIdx.x == 0) {
+      s_new = 0;
+      s_used = 0;
+    }
     const BatchTile tl = tiles[t];
     const BatchInst& I = insts[tl.inst];
     const int scap = I.scap;
@@ -588,9 +596,9 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
   // ---- per-instance group-count estimates from one sample launch ----
   B.d_insts.get(A, sizeof(BatchInst) * ninst, stream);
   ck(cudaMemcpyAsync(B.d_insts.p, B.insts.data(), sizeof(BatchInst) * ninst, cudaMemcpyHostToDevice, stream), "h2d");
-  B.d_stats.get(A, (size_t)ninst * 16, stream);
   std::vector<unsigned int> st((size_t)ninst * 4);
-  {
+  if (bo.est_groups.empty()) {
+    B.d_stats.get(A, (size_t)ninst * 16, stream);
     size_t sm = (size_t)kSampleSlots * 32;
     ck(cudaFuncSetAttribute(k_batch_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), "attr");
     k_batch_sample<<<ninst, 256, sm, stream>>>(B.P, (const BatchInst*)B.d_insts.p, (unsigned int*)B.d_stats.p);
@@ -598,6 +606,8 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
     ck(cudaMemcpyAsync(st.data(), B.d_stats.p, st.size() * 4, cudaMemcpyDeviceToHost, stream), "d2h");
     ck(cudaStreamSynchronize(stream), "sample sync");
   }
+  if (!bo.est_groups.empty() && (int)bo.est_groups.size() != ninst)
+    throw Error(ERR_LOGIC, "one group estimate per instance is required");
   B.stats.sample_s = tnow() - t_begin;
   // ---- sizing ----
   const int stride = B.P.slot_bytes;
@@ -612,7 +622,8 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
     const int64_t n = B.insts[i].n_rows;
     double d = st[i * 4 + 0], f1 = st[i * 4 + 1], m = st[i * 4 + 3];
     double est;
-    if (n <= kSampleRows) est = std::max(1.0, d);
+    if (!bo.est_groups.empty()) est = (double)std::max<int64_t>(1, bo.est_groups[i]);
+    else if (n <= kSampleRows) est = std::max(1.0, d);
     else {
       // Guaranteed-Error Estimator (Charikar et al. 2000): sqrt(n/m)*f1 + the keys
       // seen more than once; within a factor sqrt(n/m) of the truth.  The
@@ -656,7 +667,7 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
   ck(cudaFuncSetAttribute(k_batch_aggregate, cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem_bytes), "attr");
   int bps = 0;
   ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_aggregate, kBatchThreads, B.smem_bytes), "occ");
-  B.grid_agg = sms * std::max(1, bps);
+  B.grid_agg = (int)std::min<int64_t>(std::max<int64_t>(1, (int64_t)B.tiles.size()), 1 << 30);
   B.grid_compact = sms * 8;
   B.stats.instances = ninst;
   B.stats.tiles = (int64_t)B.tiles.size();
@@ -669,13 +680,16 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
   B.stats.layout_s = tnow() - t_lay;
   // trial runs: grow the tables (and outputs) of instances that overflowed
   double t_trial = tnow();
-  for (int round = 0;; ++round) {
+  for (int round = 0; bo.trial; ++round) {
     B.stats.trial_rounds = round + 1;
     B.enqueue(stream);
     ck(cudaStreamSynchronize(stream), "trial sync");
     std::vector<int> over;
-    for (int i = 0; i < ninst; ++i)
-      if (B.h_counters[(size_t)i * B.counter_words + 1]) over.push_back(i);
+    for (int i = 0; i < ninst; ++i) {
+      const unsigned int* c = B.h_counters + (size_t)i * B.counter_words;
+      // overflowed, or fuller than 0.7 (long probe runs; a later run could overflow)
+      if (c[1] || (int64_t)c[0] * 10 > B.caps[i] * 7) over.push_back(i);
+    }
     if (over.empty()) break;
     if (round >= 6) throw Error(ERR_CUDA, "batch tables keep overflowing");
     B.stats.regrown += (int64_t)over.size();
@@ -724,6 +738,21 @@ void Batch::run(cudaStream_t stream)
     if (c[1]) ++over;
   }
   B.stats.overflowed = over;
+  if (!over) return;
+  if (B.exec) throw Error(ERR_CUDA, std::to_string(over) + " batch instance table(s) overflowed; prepare the batch again");
+  // grow the overflowed tables and run again (the run is idempotent)
+  for (int round = 0; over && round < 6; ++round) {
+    for (int i = 0; i < B.ninst; ++i)
+      if (B.h_counters[(size_t)i * B.counter_words + 1]) {
+        B.caps[i] *= 4;
+        ++B.stats.regrown;
+      }
+    B.layout(stream);
+    B.enqueue(stream);
+    ck(cudaStreamSynchronize(stream), "batch sync");
+    over = 0;
+    for (int i = 0; i < B.ninst; ++i) over += B.h_counters[(size_t)i * B.counter_words + 1] ? 1 : 0;
+  }
   if (over) throw Error(ERR_CUDA, std::to_string(over) + " batch instance table(s) overflowed");
 }
 

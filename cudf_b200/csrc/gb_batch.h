@@ -11,6 +11,8 @@ struct BatchOptions {
   bool use_graph = false;  // capture the run sequence once, replay it
   int smem_bytes = 160 * 1024;
   double growth = 1.0;     // multiplies every instance's group estimate (tables size from it)
+  bool trial = true;       // run once at prepare time and regrow overflowing / overfull tables
+  std::vector<int64_t> est_groups;  // per-instance estimates from the caller (skips sampling)
 };
 
 struct BatchStats {

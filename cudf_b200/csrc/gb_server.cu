@@ -45,6 +45,7 @@ struct Query {
   int null_policy;
   double arrive, admit = 0, launch = 0, done = 0;
   int64_t est_bytes = 0;
+  int64_t est_groups = 1;
   int status = 0;  // 0 pending, 1 admitted, 2 done, 3 failed
   std::string error;
   std::shared_ptr<Batch> batch;  // keeps the result buffers alive
@@ -114,7 +115,10 @@ struct Server {
   void dispatcher()
   {
     cudaSetDevice(device);
-    cudaStreamCreateWithFlags(&sketch_stream, cudaStreamNonBlocking);
+    // the sketch must not wait behind whole batches: highest stream priority
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    cudaStreamCreateWithPriority(&sketch_stream, cudaStreamNonBlocking, hi);
     std::deque<std::shared_ptr<Query>> waiting;  // sketched, not admitted yet
     for (;;) {
       std::vector<std::shared_ptr<Query>> arrivals;
@@ -139,7 +143,10 @@ struct Server {
           for (auto& q : arrivals) q->est_bytes = -1, q->error = ex.what();
         }
         for (size_t i = 0; i < arrivals.size(); ++i) {
-          if (arrivals[i]->est_bytes == 0) arrivals[i]->est_bytes = bytes_for(*arrivals[i], est[i]);
+          if (arrivals[i]->est_bytes == 0) {
+            arrivals[i]->est_bytes = bytes_for(*arrivals[i], est[i]);
+            arrivals[i]->est_groups = (int64_t)est[i];
+          }
           waiting.push_back(arrivals[i]);
         }
       }
@@ -226,6 +233,9 @@ struct Server {
             rs.push_back(q->reqs);
           }
           BatchOptions bo;
+          bo.trial = false;  // size from the dispatcher's sketch; run() regrows on overflow
+          for (auto& q : qs) bo.est_groups.push_back(q->est_groups);
+          bo.growth = 2.0;
           b->prepare(ks, qs[0]->null_policy, rs, s, default_allocator(), bo);
           b->run(s);
         } catch (const std::exception& ex) {
