@@ -75,7 +75,8 @@ class GbServerStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("batches", ctypes.c_int64),
                 ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double), ("queries_per_s", ctypes.c_double),
                 ("peak_admitted_bytes", ctypes.c_int64), ("sketch_s", ctypes.c_double),
-                ("prepare_s", ctypes.c_double), ("run_s", ctypes.c_double), ("trial_rounds", ctypes.c_int64)]
+                ("prepare_s", ctypes.c_double), ("run_s", ctypes.c_double), ("trial_rounds", ctypes.c_int64),
+                ("direct_runs", ctypes.c_int64)]
 
 
 class GroupbyError(RuntimeError):

@@ -50,6 +50,11 @@ struct Query {
   std::string error;
   std::shared_ptr<Batch> batch;  // keeps the result buffers alive
   int index_in_batch = 0;
+  std::shared_ptr<Result> direct;  // queries run alone (large, many groups)
+  ~Query()
+  {
+    if (direct) direct->release();
+  }
 };
 
 struct WorkItem {
@@ -76,7 +81,9 @@ struct Server {
   int64_t completed = 0, failed = 0, batches = 0;
   double first_arrive = -1, last_done = 0;
   double sketch_s = 0, prepare_s = 0, run_s = 0, trial_s = 0;
-  int64_t trial_rounds = 0;
+  int64_t trial_rounds = 0, direct_runs = 0;
+  int64_t opt_direct_rows = 4 << 20;     // queries at least this long ...
+  int64_t opt_direct_groups = 4096;      // ... with more groups than this run alone
   cudaStream_t sketch_stream = nullptr;
 
   // device-side sketch of a set of queries: estimated groups per query, one
@@ -221,8 +228,48 @@ struct Server {
         }
         groups[sig].push_back(q);
       }
+      // large queries with many groups run alone through the single-query
+      // engine (its hash-partitioned path); the rest share one batched launch
+      for (auto& kv : groups) {
+        std::vector<std::shared_ptr<Query>> rest;
+        for (auto& q : kv.second) {
+          if (q->keys[0].size >= opt_direct_rows && q->est_groups > opt_direct_groups) {
+            std::string err;
+            auto R = std::make_shared<Result>();
+            try {
+              Options o;
+              o.groups_hint = q->est_groups * 2;
+              *R = aggregate(q->keys, q->null_policy, q->reqs, s, default_allocator(), o, nullptr);
+            } catch (const std::exception& ex) {
+              err = ex.what();
+            }
+            double t_done = now_s();
+            std::lock_guard<std::mutex> lk(mu);
+            q->launch = t_launch;
+            q->done = t_done;
+            if (err.empty()) {
+              q->status = 2;
+              q->direct = R;
+              ++completed;
+              ++direct_runs;
+              latencies.push_back(q->done - q->arrive);
+            } else {
+              q->status = 3;
+              q->error = err;
+              ++failed;
+              in_use -= q->est_bytes;
+            }
+            last_done = std::max(last_done, t_done);
+            cv_done.notify_all();
+          } else {
+            rest.push_back(q);
+          }
+        }
+        kv.second.swap(rest);
+      }
       for (auto& kv : groups) {
         auto& qs = kv.second;
+        if (qs.empty()) continue;
         auto b = std::make_shared<Batch>();
         std::string err;
         try {
@@ -384,9 +431,12 @@ int gb_server_wait(gb_server* sv, int64_t id, double timeout_s, gb_query_info* i
       info->queue_s = q->admit - q->arrive;
       info->num_groups = 0;
       if (q->status == 2) {
-        gb::Result R;
-        q->batch->result(q->index_in_batch, R);
-        info->num_groups = R.num_groups;
+        if (q->direct) info->num_groups = q->direct->num_groups;
+        else {
+          gb::Result R;
+          q->batch->result(q->index_in_batch, R);
+          info->num_groups = R.num_groups;
+        }
       }
     }
     if (q->status == 3) throw gb::Error(gb::ERR_CUDA, q->error);
@@ -407,7 +457,15 @@ int gb_server_result(gb_server* sv, int64_t id, int64_t* num_groups, gb_out_colu
     }
     if (q->status != 2) throw gb::Error(gb::ERR_LOGIC, "query not complete");
     gb::Result R;
-    q->batch->result(q->index_in_batch, R);
+    if (q->direct) {
+      R.num_groups = q->direct->num_groups;
+      R.keys = q->direct->keys;
+      R.results.push_back({});
+      for (auto& rc : q->direct->results)
+        for (auto& c : rc) R.results[0].push_back(c);
+    } else {
+      q->batch->result(q->index_in_batch, R);
+    }
     *num_groups = R.num_groups;
     auto put = [](gb_out_column& o, const gb::OutColumn& c) {
       o.type_id = c.type_id;
@@ -454,6 +512,7 @@ int gb_server_get_stats(gb_server* sv, gb_server_stats* out)
     out->prepare_s = S.prepare_s;
     out->run_s = S.run_s;
     out->trial_rounds = S.trial_rounds;
+    out->direct_runs = S.direct_runs;
   });
 }
 

@@ -248,6 +248,7 @@ typedef struct gb_server_stats {
   double prepare_s;           /* workers' batch sizing time (sample, layout, trial runs) */
   double run_s;               /* workers' batch run time */
   int64_t trial_rounds;
+  int64_t direct_runs;        /* large, many-group queries run alone instead of batched */
 } gb_server_stats;
 GB_API int gb_server_create(const gb_server_options* opt, gb_server** out);
 GB_API int gb_server_submit(gb_server* server, const gb_column* keys, int32_t num_keys, int32_t null_policy,

@@ -111,3 +111,23 @@ def test_invalid_query_is_rejected_at_submit():
     with pytest.raises(ValueError):
         srv.wait(12345, timeout_s=0.1)
     srv.close()
+
+
+def test_large_queries_run_alone_and_match():
+    cb, _ = _cb()
+    rng = np.random.default_rng(43)
+    qs = []
+    for n, card in ((5_000_000, 200_000), (4_500_000, 3_000_000), (200_000, 50)):
+        k = rng.integers(0, card, n).astype(np.int64)
+        qs.append((k, rng.integers(-10**6, 10**6, n).astype(np.int64), rng.normal(size=n),
+                   rng.random(n) > 0.1, rng.random(n) > 0.1))
+    dev = [_dev(q) for q in qs]
+    srv = cb.Server(workers=2)
+    ids = [srv.submit(*d) for d in dev]
+    for i, q in enumerate(qs):
+        assert srv.wait(ids[i], timeout_s=300)["status"] == 2
+        uk, res = srv.result(ids[i])
+        _check(q, uk, res)
+        srv.release(ids[i])
+    assert srv.stats()["direct_runs"] >= 1
+    srv.close()
