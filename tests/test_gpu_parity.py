@@ -262,3 +262,33 @@ def test_partitioned_skew_falls_back():
     v = rng.integers(0, 1000, n).astype(np.int64)
     run_both([cb.Column.from_numpy(key)], [(cb.Column.from_numpy(v), [agg.sum(), agg.count(), agg.max()])],
              tuning={"force_mode": 2})
+
+
+def test_distributed_groupby_single_rank_with_engine():
+    """The multi-GPU path with the engine as local aggregation (world size 1 on
+    one GPU: partial aggregate, self-exchange, merge)."""
+    import os
+    import torch.distributed as dist
+    from cudf_b200.distributed import distributed_groupby
+    from cudf_b200.types import Kind, NullPolicy
+    if not dist.is_initialized():
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29561")
+        dist.init_process_group("gloo", rank=0, world_size=1)
+    rng = np.random.default_rng(77)
+    n = 200_000
+    k = rng.integers(0, 5000, n).astype(np.int64)
+    v = rng.integers(-10**6, 10**6, n).astype(np.int64)
+    f = rng.normal(size=n)
+    m = rng.random(n) > 0.1
+    kinds = [Kind.SUM, Kind.COUNT_VALID, Kind.MIN, Kind.MAX, Kind.MEAN]
+    dev = torch.device("cuda")
+    mk, mres = distributed_groupby([(torch.from_numpy(k).to(dev), None, O.INT64)],
+                                   [((torch.from_numpy(v).to(dev), torch.from_numpy(m).to(dev), O.INT64), kinds),
+                                    ((torch.from_numpy(f).to(dev), None, O.FLOAT64), kinds)], NullPolicy.EXCLUDE)
+    o = O.groupby([O.HostColumn(O.INT64, k)], [(O.HostColumn(O.INT64, v, m), [int(x) for x in kinds]),
+                                               (O.HostColumn(O.FLOAT64, f), [int(x) for x in kinds])])
+    from parity import compare
+    gk = [(mk[0][0].cpu().numpy(), None)]
+    gr = [[(d.cpu().numpy(), None if vv is None else vv.cpu().numpy()) for d, vv in per] for per in mres]
+    compare(o, gk, gr, [[int(x) for x in kinds]] * 2, None)
