@@ -38,6 +38,20 @@ AGG_NAMES = ["sum", "count", "min", "max", "mean"]
 METRIC = "groupby rows/s (100M rows, 1M groups, 3 value cols, sum/count/min/max/mean)"
 CPU_SAMPLE_ROWS = 8_000_000
 
+# Kernels whose device time the roofline covers, by engine mode (0 global
+# table, 1 shared-memory stage, 2 hash-partitioned two-pass).
+KERNELS_BY_MODE = {0: "k_aggregate<false>", 1: "k_aggregate<true>",
+                   2: "k_part_scatter + k_part_aggregate"}
+# DRAM bytes (read + write) of those kernels per launch, from an ncu capture
+# of a smaller case of the same workload scaled up; the capture command and
+# the per-kernel figures are in profiles/.
+# Mode 2: (bytes per row, bytes per group); the partitioned copy is written
+# and read once, and the dense slots are written once per group.
+TRAFFIC_MODEL = {2: (87.07, 86.9)}
+TRAFFIC_SOURCE = {2: "ncu dram__bytes_read.sum + dram__bytes_write.sum of both kernels on the 20M-row "
+                     "case, scaled by rows (and by groups for the dense-slot writes); "
+                     "profiles/k_part_scatter_k_part_aggregate_20M.md"}
+
 
 def algorithmic_bytes(n_rows: int, n_groups: int) -> tuple[float, float]:
     """Bytes the groupby must move at least once: every input column and mask
@@ -190,8 +204,8 @@ def run_reference(args):
                                    "v2 f64, v3 f32, 10% nulls, sum/count/min/max/mean", "rows": N_ROWS,
                        "groups": N_DISTINCT, "parallelism": f"replicas{world}"},
             "cpu_baseline": {"value": v, "unit": "rows/s", "cores": threads, "kind": "port",
-                             "sample": f"first {n_sample} rows of the same generator (seed 1), "
-                                       f"oracle/gb_oracle.c with {threads} threads"},
+                             "sample": f"{n_sample} rows with the workload's distributions (numpy seed 1, "
+                                       f"1M distinct keys), oracle/gb_oracle.c with {threads} threads"},
             "e2e": {"value": v, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -250,7 +264,7 @@ def run_engine(args):
     if world > 1:
         torch.distributed.barrier()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    kernel_ms = []
+    kernel_ms, scatter_ms = [], []
     last_stats = {}
     groups = 0
     launches = 0
@@ -261,6 +275,7 @@ def run_engine(args):
             uk, res = step()
             st = gb.stats()
             kernel_ms.append(st["agg_kernel_ms"])
+            scatter_ms.append(st["scatter_ms"])
             last_stats = st
             launches += st["kernels"]
             groups = uk.num_rows()
@@ -330,7 +345,12 @@ def run_engine(args):
         peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
         inp, outb = algorithmic_bytes(n, groups)
         kmean = float(np.mean(kernel_ms)) if kernel_ms else float("nan")
+        smean = float(np.mean(scatter_ms)) if scatter_ms else 0.0
         achieved = inp / (kmean * 1e-3) / 1e9
+        mode = last_stats.get("mode", -1)
+        kname = KERNELS_BY_MODE.get(mode, "unknown")
+        tm = TRAFFIC_MODEL.get(mode)
+        traffic = None if tm is None else tm[0] * n + tm[1] * groups / world
         value = world * n / (ms * 1e-3)
         line = {
             "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
@@ -342,8 +362,12 @@ def run_engine(args):
                        "parallelism": f"rows sharded over {world} ranks, partial aggregate + NCCL all-to-all by key owner + merge" if world > 1 else "single",
                        "l2": "inputs (2.84 GB) larger than L2 (126 MB); no flush needed"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "kernel": "k_aggregate",
-                         "kernel_ms": kmean, "peak_source": peak_src,
+                         "frac": achieved / peak, "traffic": traffic, "kernel": kname,
+                         "kernel_ms": kmean, "kernel_split_ms": {"partition_scatter": smean,
+                                                                 "partition_aggregate": kmean - smean}
+                         if mode == 2 else None,
+                         "algorithmic_bytes": inp, "peak_source": peak_src,
+                         "traffic_source": TRAFFIC_SOURCE.get(mode),
                          "whole_call_frac": (inp + outb) / (ms * 1e-3) / 1e9 / peak},
             "e2e": {"value": world * n / (e_ms * 1e-3), "unit": "rows/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -355,8 +379,8 @@ def run_engine(args):
             threads = os.cpu_count() or 1
             v = cpu_reference(args.cpu_sample, threads)
             line["cpu_baseline"] = {"value": v, "unit": "rows/s", "cores": threads, "kind": "port",
-                                    "sample": f"first {args.cpu_sample} rows of the same generator "
-                                              f"(seed 1) through oracle/gb_oracle.c, {threads} threads"}
+                                    "sample": f"{args.cpu_sample} rows with the workload's distributions (numpy seed 1, "
+                                              f"1M distinct keys) through oracle/gb_oracle.c, {threads} threads"}
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
