@@ -363,7 +363,8 @@ def run_engine(args):
                        "l2": "inputs (2.84 GB) larger than L2 (126 MB); no flush needed"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": kname,
-                         "kernel_ms": kmean, "kernel_split_ms": {"partition_scatter": smean,
+                         "kernel_ms": kmean, "kernel_ms_steps": [round(x, 3) for x in kernel_ms],
+                         "kernel_split_ms": {"partition_scatter": smean,
                                                                  "partition_aggregate": kmean - smean}
                          if mode == 2 else None,
                          "algorithmic_bytes": inp, "peak_source": peak_src,

@@ -169,6 +169,10 @@ int gb_set_tuning(gb_handle* h, const gb_tuning* t)
     if (t->force_mode >= -1) o.force_mode = t->force_mode;
     if (t->groups_hint >= 0) o.groups_hint = t->groups_hint;
     if (t->profile >= 0) o.profile = t->profile;
+    if (t->scatter >= 0) {
+      if (t->scatter > 6) throw gb::Error(gb::ERR_LOGIC, "scatter must be in [0, 6]");
+      o.scatter = t->scatter;
+    }
   });
 }
 

@@ -577,6 +577,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   const int scap2 = smem_cap_for(200 * 1024);
   const int sfill2 = std::max(1, (int)(scap2 * 0.8));
   bool part_ok = !P.has_arg && !P.need_second_pass && P.num_vals <= 8 && scap2 >= 256;
+  for (int v = 0; v < P.num_vals; ++v) part_ok = part_ok && P.vals[v].basic;
   for (int a = 0; a < P.num_accs; ++a) {
     uint8_t op = P.accs[a].op;
     if (op >= OP_PROD_I64 && op <= OP_PROD_F64) part_ok = false;
@@ -664,14 +665,22 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     mark("partition scratch");
     if (opt.profile) ck(cudaEventRecord(events()[0], stream), "event");
     {
-      auto launch = [&](auto kern, int kw, int rpt) {
-        size_t psmem = part_scatter_smem(kw, rpt, nparts);
+      auto launch = [&](auto kern, int nt, int rpt) {
+        size_t psmem = part_scatter_smem(P.key_words, nt * rpt, nparts);
         ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem), "attr");
-        int grid = grid_for((const void*)kern, kScatterThreads, psmem, 0);
-        kern<<<grid, kScatterThreads, psmem, stream>>>(P, A);
+        int grid = grid_for((const void*)kern, nt, psmem, 0);
+        kern<<<grid, nt, psmem, stream>>>(P, A);
       };
-      if (P.key_words == 1) launch(k_part_scatter<1, 16>, 1, 16);
-      else launch(k_part_scatter<2, 16>, 2, 16);
+      const bool kw1 = P.key_words == 1;
+      switch (opt.scatter) {
+        case 1: kw1 ? launch(k_part_scatter<1, 16, 256, 3>, 256, 16) : launch(k_part_scatter<2, 16, 256, 3>, 256, 16); break;
+        case 2: kw1 ? launch(k_part_scatter<1, 16, 512, 2>, 512, 16) : launch(k_part_scatter<2, 16, 512, 2>, 512, 16); break;
+        case 3: kw1 ? launch(k_part_scatter<1, 8, 1024, 1>, 1024, 8) : launch(k_part_scatter<2, 8, 1024, 1>, 1024, 8); break;
+        case 4: kw1 ? launch(k_part_scatter<1, 8, 512, 3>, 512, 8) : launch(k_part_scatter<2, 8, 512, 3>, 512, 8); break;
+        case 5: kw1 ? launch(k_part_scatter<1, 4, 1024, 2, false>, 1024, 4) : launch(k_part_scatter<2, 4, 1024, 2, false>, 1024, 4); break;
+        case 6: kw1 ? launch(k_part_scatter<1, 8, 256, 4>, 256, 8) : launch(k_part_scatter<2, 8, 256, 4>, 256, 8); break;
+        default: kw1 ? launch(k_part_scatter<1, 8, 512, 3, false>, 512, 8) : launch(k_part_scatter<2, 8, 512, 3, false>, 512, 8); break;
+      }
     }
     ++st.kernels;
     ck(cudaGetLastError(), "partition launch");
@@ -688,29 +697,39 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       P2.vals[v].bit = v;
     }
     uint64_t spill_cap = 1 << 16;
+    uint32_t spill_list = 1u << 18;
     int64_t dcap = (int64_t)(est * 1.5) + (int64_t)nparts * 256 + 4096;
     for (int attempt = 0;; ++attempt) {
       T = (uint8_t*)S.get((size_t)(spill_cap + 1) * P.slot_bytes);
       dense = (uint8_t*)S.get((size_t)dcap * P.slot_bytes);
+      A.spill_rows = (int64_t*)S.get((size_t)spill_list * sizeof(int64_t));
+      A.spill_cap = spill_list;
       k_init_slots<<<dev.sms * 4, 256, 0, stream>>>(T, (int64_t)spill_cap + 1, P.slot_bytes, tmpl);
       ck(cudaMemsetAsync(counters, 0, 16, stream), "memset");
-      ck(cudaMemsetAsync(counters + 6, 0, 6 * 4, stream), "memset");  // [6] dense overflow, [8] work, [10..11] dense count
+      // [6] dense overflow, [8] work, [10..11] dense count, [12] spill list length, [13] list overflow
+      ck(cudaMemsetAsync(counters + 6, 0, 8 * 4, stream), "memset");
       G = TableRef{T, spill_cap - 1, P.slot_bytes, P.key_words, counters};
       DenseRef D{dense, dcap, (unsigned long long*)(counters + 10), counters + 6};
-      size_t sm2 = (size_t)scap2 * P.slot_bytes;
+      // shared table plus the all-ones key's slot
+      size_t sm2 = (size_t)(scap2 + 1) * P.slot_bytes;
       auto launch2 = [&](auto kern, int nt) {
         ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2), "attr");
         int grid = grid_for((const void*)kern, nt, sm2, 0);
         grid = std::min(grid, nparts);
         kern<<<grid, nt, sm2, stream>>>(P2, A, G, D, scap2, sfill2, tmpl);
       };
-      if (P.num_vals <= 4 && opt.block >= 1024) launch2(k_part_aggregate<1, 1024, 4>, 1024);
-      else launch2(k_part_aggregate<2, 512, 8>, 512);
+      const bool few = P.num_vals <= 4;
+      if (P.key_words == 1) few ? launch2(k_part_aggregate<1, 1, 1024, 4>, 1024) : launch2(k_part_aggregate<1, 1, 1024, 8>, 1024);
+      else few ? launch2(k_part_aggregate<2, 1, 1024, 4>, 1024) : launch2(k_part_aggregate<2, 1, 1024, 8>, 1024);
       if (opt.profile) ck(cudaEventRecord(events()[1], stream), "event");
+      // rows listed as not fitting their partition's table (none when the
+      // sample sized the partitions well): one grid-stride launch that reads
+      // the list length on the device
+      k_part_spill<<<dev.sms * 2, 256, 0, stream>>>(P2, G, A);
       k_finish_count<<<1, 1, 0, stream>>>(P, G);
-      st.kernels += 3;
+      st.kernels += 4;
       ck(cudaGetLastError(), "partition aggregate launch");
-      ck(cudaMemcpyAsync(host, counters, 48, cudaMemcpyDeviceToHost, stream), "d2h");
+      ck(cudaMemcpyAsync(host, counters, 64, cudaMemcpyDeviceToHost, stream), "d2h");
       ck(cudaStreamSynchronize(stream), "partition sync");
       if (opt.profile && attempt == 0) {
         float ms = 0, ms1 = 0;
@@ -721,7 +740,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       }
       mark("partition passes (synced)");
       if (host[5]) break;  // a region overflowed: fall back to the global table
-      if (host[1] == 0 && host[6] == 0) {
+      if (host[1] == 0 && host[6] == 0 && host[13] == 0) {
         done = true;
         dense_n = (int64_t)(host[10] | ((uint64_t)host[11] << 32));
         cap = spill_cap;
@@ -730,8 +749,13 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       if (attempt >= 6) throw Error(ERR_CUDA, "hash table overflow");
       if (host[1]) spill_cap *= 8;
       if (host[6]) dcap *= 2;
+      if (host[13]) {
+        spill_list = (uint32_t)std::min<uint64_t>((uint64_t)spill_list * 8, 1ull << 31);
+        spill_cap = std::max<uint64_t>(spill_cap, next_pow2((uint64_t)host[12] * 2));
+      }
       S.put(T);
       S.put(dense);
+      S.put(A.spill_rows);
       ++st.retries;
     }
     if (!done) {
@@ -740,6 +764,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       ++st.retries;
       S.put(T);
       S.put(dense);
+      S.put(A.spill_rows);
       dense = nullptr;
     }
   }

@@ -68,7 +68,7 @@ struct Result {
 
 // Engine tunables (an autotuner picks these per size bucket).
 struct Options {
-  int block = 1024;            // threads per CTA (partitioned pass 2; other kernels use at most 512)
+  int block = 512;             // threads per CTA of the global-table and shared-stage kernels
   int blocks_per_sm = 0;       // 0 = occupancy limited
   int smem_bytes = 96 * 1024;  // shared-memory table bytes per CTA (0 disables the smem stage)
   double smem_fill = 0.5;      // fraction of smem slots a CTA may claim
@@ -77,6 +77,7 @@ struct Options {
   int64_t groups_hint = -1;    // caller's group-count estimate (-1: sample)
   int force_mode = -1;         // -1 auto, 0 global only, 1 smem stage
   int profile = 0;             // time kernels with CUDA events
+  int scatter = 0;             // partitioned pass 1 launch shape (0-6: threads x rows per thread)
 };
 
 struct Stats {

@@ -29,7 +29,10 @@ struct PartArgs {
   uint64_t* keys;                // key words, key_words per row
   void* vals[kMaxValCols];       // value bits per column (column width per row)
   uint8_t* bits;                 // validity byte per row (bit v = value column v), or null
-  unsigned int* counters;        // [5] region overflow, [8] partition work counter
+  unsigned int* counters;        // [5] region overflow, [8] partition work counter,
+                                 // [12] spill list length, [13] spill list overflow
+  int64_t* spill_rows;           // pass 2: rows that did not fit their shared table
+  unsigned int spill_cap;
 };
 
 struct DenseRef {
@@ -44,172 +47,228 @@ __device__ __forceinline__ void prefetch_l2(const void* p)
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
-// Pass 1.  Each CTA takes tiles of RPT*256 rows.  A tile's rows are counting-
-// sorted by partition in shared memory (keys staged there, then each value
-// column in turn), so every (tile, partition) run leaves as one contiguous
-// write of ~tile/nparts rows instead of scattered 8-byte stores.  256 threads
-// and a 4K-row tile keep the footprint at ~64 KB so three CTAs share an SM;
-// each column's RPT loads per thread are issued back to back.
-// Shared memory: stage[tile * 8*KW] | inv u16[tile] | psort u16[tile] |
-//                hist u32[nparts] | scan u32[nparts] | gbase u64[nparts]
-constexpr int kScatterThreads = 256;
-template <int KW, int RPT>
-__global__ void __launch_bounds__(256, 3) k_part_scatter(const __grid_constant__ Plan P,
-                                                      const __grid_constant__ PartArgs A)
+// Pass 1.  Each CTA takes tiles of RPT*NT rows.  A tile's rows are counting-
+// sorted by partition in shared memory, so every (tile, partition) run leaves
+// as one contiguous write of ~tile/nparts rows instead of scattered stores:
+//   A  keys loaded (all RPT per thread at once), partition id = top hash bits,
+//      rank within the tile's partition from a shared histogram;
+//   B  one global reservation per (tile, partition) on the region cursor,
+//      exclusive scan of the histogram; per partition, `delta` maps a sorted
+//      position to its global row and `send` bounds the rows that fit;
+//   C  keys, then each value column, then the validity bytes are stored into
+//      the stage at their sorted position and written out in sorted order
+//      (consecutive threads, consecutive rows of a run).  The next column's
+//      loads are issued before the current column's write-out.
+// Shared memory: stage[tile * 8*KW] | psort u16[tile] | hist u32[nparts] |
+//                send u32[nparts] | delta i64[nparts]
+template <int KW, int RPT, int NT, int MINB, bool PF = true>
+__global__ void __launch_bounds__(NT, MINB) k_part_scatter(const __grid_constant__ Plan P,
+                                                         const __grid_constant__ PartArgs A)
 {
-  constexpr int T = kScatterThreads;
-  constexpr int TILE = RPT * T;
+  constexpr int TILE = RPT * NT;
+  static_assert(TILE <= 65536, "sorted positions are 16-bit");
   extern __shared__ __align__(16) uint8_t sh[];
   uint8_t* stage = sh;
-  uint16_t* inv = (uint16_t*)(sh + (size_t)TILE * 8 * KW);
-  uint16_t* psort = inv + TILE;
+  uint16_t* psort = (uint16_t*)(sh + (size_t)TILE * 8 * KW);
   unsigned int* hist = (unsigned int*)(psort + TILE);
-  unsigned int* scan = hist + A.nparts;
-  unsigned long long* gbase = (unsigned long long*)(scan + A.nparts + (A.nparts & 1));
-  using Scan = cub::BlockScan<unsigned, T>;
+  unsigned int* send = hist + A.nparts;
+  long long* delta = (long long*)(send + A.nparts + (A.nparts & 1));
+  using Scan = cub::BlockScan<unsigned, NT>;
   __shared__ typename Scan::TempStorage scan_tmp;
   __shared__ unsigned int s_valid;
   const int64_t n = P.num_rows;
   const bool any_bits = A.bits != nullptr;
-  const int per = (A.nparts + T - 1) / T;  // partitions per thread in the scan
+  const int nv = P.num_vals;
+  const int per = (A.nparts + NT - 1) / NT;  // partitions per thread in the scan
   for (int64_t t0 = (int64_t)blockIdx.x * TILE; t0 < n; t0 += (int64_t)gridDim.x * TILE) {
     const int cnt = (int)(n - t0 < (int64_t)TILE ? n - t0 : (int64_t)TILE);
-    for (int i = threadIdx.x; i < A.nparts; i += T) hist[i] = 0;
+    for (int i = threadIdx.x; i < A.nparts; i += NT) hist[i] = 0;
     __syncthreads();
-    // A: keys -> stage, partition ids and ranks
-    uint32_t pr[RPT];
-    if (P.num_keys == 1 && !P.keys[0].mask && P.keys[0].width == 8 && P.keys[0].cat != CAT_F64) {
-      // one plain 64-bit key: load all RPT keys first
-      const unsigned long long* kd = (const unsigned long long*)P.keys[0].data + P.keys[0].offset;
-      uint64_t kk[RPT];
+    // A
+    uint32_t pr[RPT];  // partition << 16 | rank, later partition << 16 | sorted position
+    const bool plain_key =
+      P.num_keys == 1 && !P.keys[0].mask && P.keys[0].width == 8 && P.keys[0].cat != CAT_F64;
+    const unsigned long long* kd = (const unsigned long long*)P.keys[0].data + P.keys[0].offset;
+    if (plain_key) {
+      // one plain 64-bit key: its bits are the key word
+      uint64_t k0[RPT];
 #pragma unroll
       for (int k = 0; k < RPT; ++k) {
-        int i = k * T + threadIdx.x;
-        kk[k] = i < cnt ? __ldg(kd + t0 + i) : 0;
+        const int i = k * NT + threadIdx.x;
+        k0[k] = i < cnt ? __ldg(kd + t0 + i) : 0;
       }
 #pragma unroll
       for (int k = 0; k < RPT; ++k) {
-        int i = k * T + threadIdx.x;
+        const int i = k * NT + threadIdx.x;
         pr[k] = 0xFFFFFFFFu;
         if (i < cnt) {
-          ((uint64_t*)stage)[i] = kk[k];
-          unsigned p = (unsigned)(hash_key(kk[k], 0, 1) >> A.shift);
+          const unsigned p = (unsigned)(hash_key(k0[k], 0, 1) >> A.shift);
           pr[k] = (p << 16) | atomicAdd(&hist[p], 1u);
         }
       }
     } else {
 #pragma unroll
       for (int k = 0; k < RPT; ++k) {
-        int i = k * T + threadIdx.x;
+        const int i = k * NT + threadIdx.x;
         pr[k] = 0xFFFFFFFFu;
-        uint64_t w0, w1;
+        uint64_t w0 = 0, w1 = 0;
         if (i < cnt && pack_key(P, t0 + i, w0, w1)) {
-          if (KW == 1) ((uint64_t*)stage)[i] = w0;
-          else ((ulonglong2*)stage)[i] = make_ulonglong2(w0, w1);
-          unsigned p = (unsigned)(hash_key(w0, w1, KW) >> A.shift);
+          const unsigned p = (unsigned)(hash_key(w0, w1, KW) >> A.shift);
           pr[k] = (p << 16) | atomicAdd(&hist[p], 1u);
         }
       }
     }
     __syncthreads();
-    // B: reserve each partition's run; exclusive scan of the histogram
+    // B: reservations (independent atomics, issued before their results are
+    // used), then the scan
     unsigned mine = 0;
-    for (int q = threadIdx.x * per; q < min(A.nparts, (threadIdx.x + 1) * per); ++q) {
-      unsigned h = hist[q];
-      mine += h;
-      if (h) {
-        unsigned long long g = atomicAdd(&A.cursor[q], (unsigned long long)h);
-        gbase[q] = g;
-        if ((int64_t)(g + h) > A.end[q]) atomicOr(A.counters + 5, 1u);
+    for (int q0 = threadIdx.x * per; q0 < min(A.nparts, (threadIdx.x + 1) * per); q0 += 4) {
+      unsigned h[4];
+      unsigned long long g[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int q = q0 + j;
+        h[j] = (j < per && q < min(A.nparts, (threadIdx.x + 1) * per)) ? hist[q] : 0u;
+        g[j] = h[j] ? atomicAdd(&A.cursor[q], (unsigned long long)h[j]) : 0ull;
+        mine += h[j];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int q = q0 + j;
+        if (!h[j]) continue;
+        const long long room = (long long)A.end[q] - (long long)g[j];
+        if ((long long)h[j] > room) atomicOr(A.counters + 5, 1u);
+        delta[q] = (long long)g[j];                      // minus the scan offset below
+        send[q] = room <= 0 ? 0u : (unsigned)min((long long)h[j], room);  // plus the offset below
       }
     }
     unsigned off, total;
     Scan(scan_tmp).ExclusiveSum(mine, off, total);
     for (int q = threadIdx.x * per; q < min(A.nparts, (threadIdx.x + 1) * per); ++q) {
-      scan[q] = off;
-      off += hist[q];
+      const unsigned h = hist[q];
+      if (h) {
+        delta[q] -= (long long)off;
+        send[q] += off;
+      }
+      hist[q] = off;  // partition start in the sorted tile
+      off += h;
     }
     if (threadIdx.x == 0) s_valid = total;
     __syncthreads();
-    // C: sorted order
+    const int nvalid = (int)s_valid;
+    // C: sorted positions; keys (read again: the tile was just loaded, so
+    // they come from cache) through the stage
 #pragma unroll
     for (int k = 0; k < RPT; ++k) {
       if (pr[k] == 0xFFFFFFFFu) continue;
-      unsigned p = pr[k] >> 16;
-      unsigned s = scan[p] + (pr[k] & 0xFFFFu);
-      inv[s] = (uint16_t)(k * T + threadIdx.x);
+      const unsigned p = pr[k] >> 16;
+      const unsigned s = hist[p] + (pr[k] & 0xFFFFu);
+      pr[k] = (p << 16) | s;
       psort[s] = (uint16_t)p;
     }
-    __syncthreads();
-    const int nvalid = (int)s_valid;
-    // D: keys out
-    for (int s = threadIdx.x; s < nvalid; s += T) {
-      unsigned p = psort[s];
-      int64_t g = (int64_t)gbase[p] + (s - (int)scan[p]);
-      if (g >= A.end[p]) continue;
-      if (KW == 1) A.keys[g] = ((const uint64_t*)stage)[inv[s]];
-      else ((ulonglong2*)A.keys)[g] = ((const ulonglong2*)stage)[inv[s]];
-    }
-    // E: each value column through the stage
-    uint32_t vb[RPT];
+    if (plain_key) {
+      uint64_t k0[RPT];
 #pragma unroll
-    for (int k = 0; k < RPT; ++k) vb[k] = 0;
-#pragma unroll 1
-    for (int v = 0; v < P.num_vals; ++v) {
-      const ValCol& c = P.vals[v];
-      uint64_t x[RPT];
-#pragma unroll
-      for (int k = 0; k < RPT; ++k) {
-        int i = k * T + threadIdx.x;
-        x[k] = pr[k] != 0xFFFFFFFFu ? load_bits(c.data, t0 + i + c.offset, c.width) : 0;
-      }
-      if (any_bits && c.mask) {
-#pragma unroll
-        for (int k = 0; k < RPT; ++k)
-          if (pr[k] != 0xFFFFFFFFu && bit_valid(c.mask, t0 + k * T + threadIdx.x + c.offset)) vb[k] |= 1u << v;
-      } else if (any_bits) {
-#pragma unroll
-        for (int k = 0; k < RPT; ++k) vb[k] |= 1u << v;
-      }
-      __syncthreads();
+      for (int k = 0; k < RPT; ++k) k0[k] = pr[k] != 0xFFFFFFFFu ? __ldg(kd + t0 + k * NT + threadIdx.x) : 0;
 #pragma unroll
       for (int k = 0; k < RPT; ++k)
-        if (pr[k] != 0xFFFFFFFFu) store_width(stage, k * T + threadIdx.x, c.width, x[k]);
+        if (pr[k] != 0xFFFFFFFFu) ((uint64_t*)stage)[pr[k] & 0xFFFFu] = k0[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        if (pr[k] == 0xFFFFFFFFu) continue;
+        uint64_t w0 = 0, w1 = 0;
+        pack_key(P, t0 + k * NT + threadIdx.x, w0, w1);
+        if (KW == 1) ((uint64_t*)stage)[pr[k] & 0xFFFFu] = w0;
+        else ((ulonglong2*)stage)[pr[k] & 0xFFFFu] = make_ulonglong2(w0, w1);
+      }
+    }
+    // first value column's loads in flight with the key write-out
+    uint64_t x[RPT];
+    auto load_col = [&](int v) {
+      const ValCol& c = P.vals[v];
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int i = k * NT + threadIdx.x;
+        x[k] = pr[k] != 0xFFFFFFFFu ? load_bits(c.data, t0 + i + c.offset, c.width) : 0;
+      }
+    };
+    if (PF && nv > 0) load_col(0);
+    __syncthreads();
+    for (int s = threadIdx.x; s < nvalid; s += NT) {
+      const unsigned p = psort[s];
+      if ((unsigned)s >= send[p]) continue;
+      const int64_t g = delta[p] + s;
+      if (KW == 1) A.keys[g] = ((const uint64_t*)stage)[s];
+      else ((ulonglong2*)A.keys)[g] = ((const ulonglong2*)stage)[s];
+    }
+    // validity bytes of this thread's rows, four to a register
+    uint32_t vb[(RPT + 3) / 4];
+#pragma unroll
+    for (int k = 0; k < (RPT + 3) / 4; ++k) vb[k] = 0;
+#pragma unroll 1
+    for (int v = 0; v < nv; ++v) {
+      const ValCol& c = P.vals[v];
+      if (any_bits) {
+#pragma unroll
+        for (int k = 0; k < RPT; ++k)
+          if (pr[k] != 0xFFFFFFFFu && (!c.mask || bit_valid(c.mask, t0 + k * NT + threadIdx.x + c.offset)))
+            vb[k >> 2] |= 1u << (v + 8 * (k & 3));
+      }
+      if (!PF) load_col(v);
+      __syncthreads();  // the previous write-out has read the stage
+#pragma unroll
+      for (int k = 0; k < RPT; ++k)
+        if (pr[k] != 0xFFFFFFFFu) store_width(stage, pr[k] & 0xFFFFu, c.width, x[k]);
       __syncthreads();
-      for (int s = threadIdx.x; s < nvalid; s += T) {
-        unsigned p = psort[s];
-        int64_t g = (int64_t)gbase[p] + (s - (int)scan[p]);
-        if (g >= A.end[p]) continue;
-        int i = inv[s];
-        switch (c.width) {
-          case 1: ((uint8_t*)A.vals[v])[g] = stage[i]; break;
-          case 2: ((uint16_t*)A.vals[v])[g] = ((const uint16_t*)stage)[i]; break;
-          case 4: ((uint32_t*)A.vals[v])[g] = ((const uint32_t*)stage)[i]; break;
-          default: ((uint64_t*)A.vals[v])[g] = ((const uint64_t*)stage)[i]; break;
-        }
+      if (PF && v + 1 < nv) load_col(v + 1);
+      void* dst = A.vals[v];
+      switch (c.width) {
+        case 8:
+          for (int s = threadIdx.x; s < nvalid; s += NT) {
+            const unsigned p = psort[s];
+            if ((unsigned)s < send[p]) ((uint64_t*)dst)[delta[p] + s] = ((const uint64_t*)stage)[s];
+          }
+          break;
+        case 4:
+          for (int s = threadIdx.x; s < nvalid; s += NT) {
+            const unsigned p = psort[s];
+            if ((unsigned)s < send[p]) ((uint32_t*)dst)[delta[p] + s] = ((const uint32_t*)stage)[s];
+          }
+          break;
+        case 2:
+          for (int s = threadIdx.x; s < nvalid; s += NT) {
+            const unsigned p = psort[s];
+            if ((unsigned)s < send[p]) ((uint16_t*)dst)[delta[p] + s] = ((const uint16_t*)stage)[s];
+          }
+          break;
+        default:
+          for (int s = threadIdx.x; s < nvalid; s += NT) {
+            const unsigned p = psort[s];
+            if ((unsigned)s < send[p]) ((uint8_t*)dst)[delta[p] + s] = stage[s];
+          }
+          break;
       }
     }
     if (any_bits) {
       __syncthreads();
 #pragma unroll
       for (int k = 0; k < RPT; ++k)
-        if (pr[k] != 0xFFFFFFFFu) stage[k * T + threadIdx.x] = (uint8_t)vb[k];
+        if (pr[k] != 0xFFFFFFFFu) stage[pr[k] & 0xFFFFu] = (uint8_t)(vb[k >> 2] >> (8 * (k & 3)));
       __syncthreads();
-      for (int s = threadIdx.x; s < nvalid; s += T) {
-        unsigned p = psort[s];
-        int64_t g = (int64_t)gbase[p] + (s - (int)scan[p]);
-        if (g < A.end[p]) A.bits[g] = stage[inv[s]];
+      for (int s = threadIdx.x; s < nvalid; s += NT) {
+        const unsigned p = psort[s];
+        if ((unsigned)s < send[p]) A.bits[delta[p] + s] = stage[s];
       }
     }
     __syncthreads();
   }
 }
 
-// shared-memory bytes k_part_scatter<KW, RPT> needs
-inline size_t part_scatter_smem(int kw, int rpt, int nparts)
+// shared-memory bytes of k_part_scatter for a tile of `tile` rows
+inline size_t part_scatter_smem(int kw, int tile, int nparts)
 {
-  size_t tile = (size_t)rpt * kScatterThreads;
-  return tile * 8 * kw + tile * 4 + (size_t)nparts * 8 + 8 + (size_t)nparts * 8;
+  return (size_t)tile * 8 * kw + (size_t)tile * 2 + (size_t)nparts * 8 + 8 + (size_t)nparts * 8;
 }
 
 // Shared-memory find-or-insert (bounded probes); null when the key does not
@@ -274,120 +333,39 @@ __device__ __forceinline__ uint64_t sld_u64(uint32_t a)
   return v;
 }
 
-// Ops the partitioned path supports (PRODUCT and ARGMIN/ARGMAX plans use the
-// other modes).
-__device__ __forceinline__ bool part_op_ok(uint8_t op)
+// Rows whose key did not fit their partition's shared table (a partition
+// with more groups than the sample predicted) are listed by pass 2 and
+// applied to the global spill table afterwards by k_part_spill, so the hot
+// loop carries no call into the generic update code.  The list count lives in
+// counters[12]; counters[13] is set when the list itself overflowed (the host
+// then re-runs pass 2 with a longer list).
+static __global__ void __launch_bounds__(256) k_part_spill(const __grid_constant__ Plan P2, TableRef G,
+                                                           const __grid_constant__ PartArgs A)
 {
-  return op <= OP_MAX_U64 || op == OP_SQ_I64 || op == OP_SQ_F32 || op == OP_SQ_F64;
-}
-
-// Applies one valid value (raw bits) of column c to a shared slot at `sa`.
-__device__ __noinline__ void sapply(const Plan& P, const ValCol& c, uint32_t sa, uint64_t bits)
-{
-  int64_t iv = 0;
-  float f = 0.f;
-  double d = 0.0;
-  switch (c.cat) {
-    case CAT_SIGNED: iv = sign_extend(bits, c.width); break;
-    case CAT_BOOL: iv = bits != 0; break;
-    case CAT_UNSIGNED: iv = (int64_t)bits; break;
-    case CAT_F32: f = __uint_as_float((uint32_t)bits); d = f; break;
-    default: d = __longlong_as_double((long long)bits); break;
-  }
-#pragma unroll 1
-  for (int a = c.acc_begin; a < c.acc_end; ++a) {
-    const Acc A = P.accs[a];
-    uint32_t p = sa + A.off;
-    switch (A.op) {
-      case OP_SUM_I64: sred_add_u64(p, (uint64_t)iv); break;
-      case OP_SUM_I32: sred_add_u32(p, (uint32_t)iv); break;
-      case OP_SUM_F32: sred_add_f32(p, f); break;
-      case OP_SUM_F64: sred_add_f64(p, d); break;
-      case OP_MIN_U32: case OP_MAX_U32: {
-        bool mn = A.op == OP_MIN_U32;
-        uint32_t v = c.cat == CAT_F32 ? ord32_f(f, mn)
-                     : (c.cat == CAT_UNSIGNED || c.cat == CAT_BOOL) ? (uint32_t)iv
-                                                                    : ((uint32_t)(int32_t)iv ^ 0x80000000u);
-        uint32_t cur = sld_u32(p);
-        if (mn ? v < cur : v > cur) { if (mn) sred_min_u32(p, v); else sred_max_u32(p, v); }
-        break;
-      }
-      case OP_MIN_U64: case OP_MAX_U64: {
-        bool mn = A.op == OP_MIN_U64;
-        uint64_t v = c.cat == CAT_F64 ? ord64_f(d, mn)
-                     : c.cat == CAT_UNSIGNED ? bits : ((uint64_t)iv ^ 0x8000000000000000ull);
-        uint64_t cur = sld_u64(p);
-        if (mn ? v < cur : v > cur) { if (mn) sred_min_u64(p, v); else sred_max_u64(p, v); }
-        break;
-      }
-      case OP_SQ_I64: sred_add_u64(p, (uint64_t)iv * (uint64_t)iv); break;
-      case OP_SQ_F32: sred_add_f32(p, f * f); break;
-      case OP_SQ_F64: sred_add_f64(p, d * d); break;
-      default: break;
+  __shared__ unsigned int s_new;
+  if (threadIdx.x == 0) s_new = 0;
+  __syncthreads();
+  const unsigned cnt = min(*(volatile unsigned int*)(A.counters + 12), A.spill_cap);
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    const int64_t r = A.spill_rows[i];
+    const uint64_t w0 = P2.packed_keys[r * P2.key_words];
+    const uint64_t w1 = P2.key_words == 2 ? P2.packed_keys[r * 2 + 1] : 0;
+    const uint64_t h = hash_key(w0, w1, P2.key_words);
+    const int64_t gi = global_slot(P2, G, w0, w1, h, &s_new);
+    if (gi < 0) {
+      atomicOr(G.counters + 1, 1u);
+      continue;
     }
+    update_slot(P2, G.T + gi * (int64_t)G.stride, r);
   }
-}
-
-// Same as sapply for a column whose accumulators are only SUM/MIN/MAX/sum of
-// squares: the value is converted once and each accumulator is a fixed
-// offset, without the per-accumulator dispatch.
-__device__ __forceinline__ void sapply_basic(const ValCol& c, uint32_t sa, uint64_t bits)
-{
-  const uint8_t cat = c.cat;
-  int64_t iv = 0;
-  float f = 0.f;
-  double d = 0.0;
-  if (cat == CAT_F32) { f = __uint_as_float((uint32_t)bits); d = f; }
-  else if (cat == CAT_F64) d = __longlong_as_double((long long)bits);
-  else if (cat == CAT_SIGNED) iv = sign_extend(bits, c.width);
-  else if (cat == CAT_BOOL) iv = bits != 0;
-  else iv = (int64_t)bits;
-  switch (c.sum_op) {
-    case OP_SUM_I64: sred_add_u64(sa + c.sum_off, (uint64_t)iv); break;
-    case OP_SUM_I32: sred_add_u32(sa + c.sum_off, (uint32_t)iv); break;
-    case OP_SUM_F32: sred_add_f32(sa + c.sum_off, f); break;
-    case OP_SUM_F64: sred_add_f64(sa + c.sum_off, d); break;
-    default: break;
-  }
-  if (c.min_off >= 0 || c.max_off >= 0) {
-    if (c.width == 8) {
-      uint64_t lo, hi;
-      if (cat == CAT_F64) { lo = ord64_f(d, true); hi = ord64_f(d, false); }
-      else if (cat == CAT_UNSIGNED) lo = hi = bits;
-      else lo = hi = (uint64_t)iv ^ 0x8000000000000000ull;
-      if (c.min_off >= 0) sred_min_u64(sa + c.min_off, lo);
-      if (c.max_off >= 0) sred_max_u64(sa + c.max_off, hi);
-    } else {
-      uint32_t lo, hi;
-      if (cat == CAT_F32) { lo = ord32_f(f, true); hi = ord32_f(f, false); }
-      else if (cat == CAT_UNSIGNED || cat == CAT_BOOL) lo = hi = (uint32_t)iv;
-      else lo = hi = (uint32_t)(int32_t)iv ^ 0x80000000u;
-      if (c.min_off >= 0) sred_min_u32(sa + c.min_off, lo);
-      if (c.max_off >= 0) sred_max_u32(sa + c.max_off, hi);
-    }
-  }
-  if (c.sq_off >= 0) {
-    if (cat == CAT_F32) sred_add_f32(sa + c.sq_off, f * f);
-    else if (cat == CAT_F64) sred_add_f64(sa + c.sq_off, d * d);
-    else sred_add_u64(sa + c.sq_off, (uint64_t)iv * (uint64_t)iv);
-  }
-}
-
-// A row whose key did not fit the shared table: global table, generic update.
-__device__ __noinline__ void spill_row(const Plan& P2, const TableRef& G, uint64_t w0, uint64_t w1,
-                                       uint64_t h, int64_t r, unsigned int* s_new)
-{
-  int64_t gi = global_slot(P2, G, w0, w1, h, s_new);
-  if (gi < 0) {
-    atomicOr(G.counters + 1, 1u);
-    return;
-  }
-  update_slot(P2, G.T + gi * (int64_t)G.stride, r);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_new) atomicAdd(G.counters, s_new);
 }
 
 // ---- pass 2 ----
-// Per-partition prologue: claim a partition, reset the shared table.  Returns
-// the partition id (>= nparts: no work left).
+// Per-partition prologue: claim a partition, reset the shared table (`scap`
+// slots plus, for one-word keys, the slot of the all-ones key).  Returns the
+// partition id (>= nparts: no work left).
 template <int NT>
 __device__ __forceinline__ int p2_claim(const PartArgs& A, uint8_t* smem, int scap, int nw,
                                         const SlotTemplate& tmpl, int* s_part, unsigned int* s_used,
@@ -407,7 +385,9 @@ __device__ __forceinline__ int p2_claim(const PartArgs& A, uint8_t* smem, int sc
 }
 
 // Per-partition epilogue: the partition's groups leave as dense slots, or are
-// merged into the global spill table when some of its rows went there.
+// merged into the global spill table when some of its rows went there.  The
+// all-ones key's slot (one-word keys; it cannot be told from an empty slot)
+// is always merged into the global table's dedicated slot.
 template <int NT, typename ScanT>
 __device__ __forceinline__ void p2_flush(const Plan& P2, const TableRef& G, const DenseRef& D,
                                          const uint8_t* smem, int scap, bool spilled,
@@ -416,6 +396,10 @@ __device__ __forceinline__ void p2_flush(const Plan& P2, const TableRef& G, cons
 {
   const int stride = G.stride;
   const int nw = stride / 8;
+  if (P2.key_words == 1 && threadIdx.x == 0) {
+    const uint8_t* sp = smem + (size_t)scap * stride;
+    if (*(const uint32_t*)(sp + P2.rows_off) > 0) merge_slot(P2, G, sp, s_new);
+  }
   if (spilled) {
     for (int i = threadIdx.x; i < scap; i += NT) {
       const uint8_t* s = smem + i * stride;
@@ -445,13 +429,77 @@ __device__ __forceinline__ void p2_flush(const Plan& P2, const TableRef& G, cons
   }
 }
 
+// One value column of a chunk of R rows per thread (values already loaded),
+// with the column's type fixed at compile time: each accumulator present
+// (sum, min, max, sum of squares) is one shared-memory reduction per row.
+// `ok` = 0 marks rows that are absent, null in this column, or were listed
+// as spills.
+template <int CAT, int W, int R, int MAXV>
+__device__ __forceinline__ void p2_column(const ValCol& c, const uint32_t (&sa)[R], const uint32_t (&ok)[R],
+                                          const uint64_t (&xv)[R][MAXV], int v)
+{
+  uint64_t x[R];
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    x[j] = 0;
+#pragma unroll
+    for (int u = 0; u < MAXV; ++u)
+      if (u == v) x[j] = xv[j][u];
+  }
+  const int so = c.sum_off, mo = c.min_off, xo = c.max_off, qo = c.sq_off;
+  const bool sum32 = c.sum_op == OP_SUM_I32;
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    if (!ok[j]) continue;
+    const uint32_t a = sa[j];
+    if (CAT == CAT_F64) {
+      const double d = __longlong_as_double((long long)x[j]);
+      if (so >= 0) sred_add_f64(a + so, d);
+      if (mo >= 0) sred_min_u64(a + mo, ord64_f(d, true));
+      if (xo >= 0) sred_max_u64(a + xo, ord64_f(d, false));
+      if (qo >= 0) sred_add_f64(a + qo, d * d);
+    } else if (CAT == CAT_F32) {
+      const float f = __uint_as_float((uint32_t)x[j]);
+      if (so >= 0) sred_add_f32(a + so, f);
+      if (mo >= 0) sred_min_u32(a + mo, ord32_f(f, true));
+      if (xo >= 0) sred_max_u32(a + xo, ord32_f(f, false));
+      if (qo >= 0) sred_add_f32(a + qo, f * f);
+    } else {
+      // integers: sign- or zero-extended to 64 bits; min/max in the
+      // order-preserving unsigned encoding of the slot's width
+      int64_t iv;
+      if (CAT == CAT_SIGNED) iv = W == 8 ? (int64_t)x[j] : W == 4 ? (int64_t)(int32_t)x[j]
+                                        : W == 2 ? (int64_t)(int16_t)x[j] : (int64_t)(int8_t)x[j];
+      else if (CAT == CAT_BOOL) iv = x[j] != 0;
+      else iv = (int64_t)x[j];
+      if (so >= 0) {
+        if (sum32) sred_add_u32(a + so, (uint32_t)iv);
+        else sred_add_u64(a + so, (uint64_t)iv);
+      }
+      if (W == 8) {
+        const uint64_t o = CAT == CAT_SIGNED ? ((uint64_t)iv ^ 0x8000000000000000ull) : (uint64_t)iv;
+        if (mo >= 0) sred_min_u64(a + mo, o);
+        if (xo >= 0) sred_max_u64(a + xo, o);
+      } else {
+        const uint32_t o = CAT == CAT_SIGNED ? ((uint32_t)(int32_t)iv ^ 0x80000000u) : (uint32_t)iv;
+        if (mo >= 0) sred_min_u32(a + mo, o);
+        if (xo >= 0) sred_max_u32(a + xo, o);
+      }
+      if (qo >= 0) sred_add_u64(a + qo, (uint64_t)iv * (uint64_t)iv);
+    }
+  }
+}
+
 // Pass 2.  P2 is the plan with value columns redirected to the partitioned
 // arrays (offset 0, `bits` validity) and packed_keys set.  One CTA owns a
-// partition at a time and aggregates it in a shared-memory table.  The row
-// loop is software-pipelined: while step t's rows are placed in the table,
-// step t's values (every column) and step t+1's keys are already in flight,
-// and step t+2 is prefetched into L2.  MAXV bounds the value columns.
-template <int R, int NT, int MAXV>
+// partition at a time and aggregates it in a shared-memory table.  Rows are
+// taken in chunks of R per thread: the chunk's keys are placed in the table
+// (the next chunk's keys and validity bytes are loaded meanwhile, and the
+// chunk after that is prefetched into L2, each thread owning one fixed
+// 128-byte line of the key, value and validity arrays), then the columns are
+// applied one at a time, each through code specialised for its type, so the
+// per-type dispatch happens once per column and chunk instead of per row.
+template <int KW, int R, int NT, int MAXV>
 __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant__ Plan P2,
                                                           const __grid_constant__ PartArgs A,
                                                           TableRef G, DenseRef D, int scap, int sfill,
@@ -469,25 +517,42 @@ __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant_
   const uint64_t smask = (uint64_t)scap - 1;
   const bool have_bits = A.bits != nullptr;
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
-  const int kw = P2.key_words;
   const int nv = P2.num_vals;
+  constexpr int64_t STEP = (int64_t)R * NT;
+  // this thread's prefetch line: array base, bytes per row, byte offset in a step
+  const uint8_t* pf_base = nullptr;
+  int pf_w = 0, pf_off = 0;
+  {
+    int line = threadIdx.x;
+    auto take = [&](const void* base, int w) {
+      const int lines = (int)((STEP * w + 127) / 128);
+      if (pf_base == nullptr && line >= 0 && line < lines) {
+        pf_base = (const uint8_t*)base;
+        pf_w = w;
+        pf_off = line * 128;
+      }
+      line -= lines;
+    };
+    take(P2.packed_keys, 8 * KW);
+    for (int v = 0; v < nv; ++v) take(P2.vals[v].data, P2.vals[v].width);
+    if (have_bits) take(A.bits, 1);
+  }
   for (;;) {
-    const int p = p2_claim<NT>(A, smem, scap, nw, tmpl, &s_part, &s_used, &s_spill);
+    const int p = p2_claim<NT>(A, smem, scap + (KW == 1), nw, tmpl, &s_part, &s_used, &s_spill);
     if (p >= A.nparts) break;
     const int64_t b = A.base[p];
     const int64_t e = min((int64_t)A.cursor[p], A.end[p]);
-    constexpr int64_t STEP = (int64_t)R * NT;
     auto load_keys = [&](int64_t r0, uint64_t (&k0)[R], uint64_t (&k1)[R], uint32_t (&vb)[R]) {
 #pragma unroll
       for (int j = 0; j < R; ++j) {
-        int64_t r = r0 + (int64_t)j * NT + threadIdx.x;
+        const int64_t r = r0 + (int64_t)j * NT + threadIdx.x;
         k0[j] = kEmpty;
         k1[j] = 0;
         vb[j] = 0xFFFFFFFFu;
         if (r < e) {
-          if (kw == 1) k0[j] = __ldg(P2.packed_keys + r);
+          if (KW == 1) k0[j] = __ldg(P2.packed_keys + r);
           else {
-            ulonglong2 kk = __ldg((const ulonglong2*)(P2.packed_keys + 2 * r));
+            const ulonglong2 kk = __ldg((const ulonglong2*)(P2.packed_keys + 2 * r));
             k0[j] = kk.x;
             k1[j] = kk.y;
           }
@@ -498,74 +563,73 @@ __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant_
     uint64_t k0[R], k1[R];
     uint32_t vb[R];
     load_keys(b, k0, k1, vb);
+    const int64_t pf_end = e * pf_w;
     for (int64_t r0 = b; r0 < e; r0 += STEP) {
-      // step t+2 into L2
-      {
-        const int64_t n0 = r0 + 2 * STEP;
-        const int64_t n1 = min(e, n0 + STEP);
-        if (n0 < n1) {
-          const int64_t t = threadIdx.x;
-          if (t * 128 < (n1 - n0) * 8 * kw) prefetch_l2((const uint8_t*)(P2.packed_keys + n0 * kw) + t * 128);
-#pragma unroll
-          for (int v = 0; v < MAXV; ++v) {
-            if (v >= nv) break;
-            if (t * 128 < (n1 - n0) * P2.vals[v].width)
-              prefetch_l2((const uint8_t*)P2.vals[v].data + n0 * P2.vals[v].width + t * 128);
-          }
-          if (have_bits && t * 128 < n1 - n0) prefetch_l2(A.bits + n0 + t * 128);
-        }
+      if (pf_base) {
+        const int64_t at = (r0 + 2 * STEP) * pf_w + pf_off;
+        if (at < pf_end) prefetch_l2(pf_base + at);
       }
-      // place this step's rows
+      // place this chunk's rows
       uint32_t sa[R];
+      int64_t row[R];
 #pragma unroll
       for (int j = 0; j < R; ++j) {
-        int64_t r = r0 + (int64_t)j * NT + threadIdx.x;
+        row[j] = r0 + (int64_t)j * NT + threadIdx.x;
         sa[j] = 0;
-        if (r >= e) continue;
-        uint64_t h = hash_key(k0[j], k1[j], kw);
-        uint8_t* slot = smem_slot(smem, stride, smask, sfill, &s_used, kw, k0[j], k1[j], h);
+        if (row[j] >= e) continue;
+        const uint64_t h = hash_key(k0[j], k1[j], KW);
+        uint8_t* slot = (KW == 1 && k0[j] == kEmpty)
+                          ? smem + (size_t)scap * stride
+                          : smem_slot(smem, stride, smask, sfill, &s_used, KW, k0[j], k1[j], h);
         if (slot == nullptr) {
           s_spill = 1;
-          spill_row(P2, G, k0[j], k1[j], h, r, &s_new);
+          const unsigned at = atomicAdd(A.counters + 12, 1u);
+          if (at < A.spill_cap) A.spill_rows[at] = row[j];
+          else atomicOr(A.counters + 13, 1u);
           continue;
         }
         sa[j] = sbase + (uint32_t)(slot - smem);
-      }
-      // this step's values and the next step's keys in flight together
-      uint64_t x[R][MAXV];
-#pragma unroll
-      for (int j = 0; j < R; ++j) {
-        int64_t r = r0 + (int64_t)j * NT + threadIdx.x;
-#pragma unroll
-        for (int v = 0; v < MAXV; ++v) {
-          x[j][v] = 0;
-          if (v < nv && sa[j] && ((vb[j] >> v) & 1)) x[j][v] = load_bits(P2.vals[v].data, r, P2.vals[v].width);
-        }
-      }
-      uint64_t nk0[R], nk1[R];
-      uint32_t nvb[R];
-      load_keys(r0 + STEP, nk0, nk1, nvb);
-#pragma unroll
-      for (int j = 0; j < R; ++j) {
-        if (!sa[j]) continue;
         sred_add_u32(sa[j] + P2.rows_off, 1u);
-#pragma unroll
-        for (int v = 0; v < MAXV; ++v) {
-          if (v >= nv) break;
-          const ValCol& c = P2.vals[v];
-          if (!((vb[j] >> v) & 1)) {
-            if (c.nulls_off >= 0) sred_add_u32(sa[j] + c.nulls_off, 1u);
-            continue;
-          }
-          if (c.basic) sapply_basic(c, sa[j], x[j][v]);
-          else sapply(P2, c, sa[j], x[j][v]);
-        }
       }
+      uint32_t cur_vb[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j) cur_vb[j] = vb[j];
+      // every column's values of this chunk, and the next chunk's keys, in
+      // flight together
+      uint64_t xv[R][MAXV];
 #pragma unroll
       for (int j = 0; j < R; ++j) {
-        k0[j] = nk0[j];
-        k1[j] = nk1[j];
-        vb[j] = nvb[j];
+#pragma unroll
+        for (int v = 0; v < MAXV; ++v) {
+          xv[j][v] = 0;
+          if (v < nv && sa[j] && ((cur_vb[j] >> v) & 1)) xv[j][v] = load_bits(P2.vals[v].data, row[j], P2.vals[v].width);
+        }
+      }
+      load_keys(r0 + STEP, k0, k1, vb);
+#pragma unroll
+      for (int v = 0; v < MAXV; ++v) {
+        if (v >= nv) break;
+        const ValCol& c = P2.vals[v];
+        uint32_t ok[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          const bool valid = (cur_vb[j] >> v) & 1;
+          ok[j] = sa[j] != 0 && valid;
+          if (sa[j] != 0 && !valid && c.nulls_off >= 0) sred_add_u32(sa[j] + c.nulls_off, 1u);
+        }
+        switch ((c.cat << 4) | c.width) {
+          case (CAT_F64 << 4) | 8: p2_column<CAT_F64, 8, R, MAXV>(c, sa, ok, xv, v); break;
+          case (CAT_F32 << 4) | 4: p2_column<CAT_F32, 4, R, MAXV>(c, sa, ok, xv, v); break;
+          case (CAT_SIGNED << 4) | 8: p2_column<CAT_SIGNED, 8, R, MAXV>(c, sa, ok, xv, v); break;
+          case (CAT_SIGNED << 4) | 4: p2_column<CAT_SIGNED, 4, R, MAXV>(c, sa, ok, xv, v); break;
+          case (CAT_SIGNED << 4) | 2: p2_column<CAT_SIGNED, 2, R, MAXV>(c, sa, ok, xv, v); break;
+          case (CAT_SIGNED << 4) | 1: p2_column<CAT_SIGNED, 1, R, MAXV>(c, sa, ok, xv, v); break;
+          case (CAT_UNSIGNED << 4) | 8: p2_column<CAT_UNSIGNED, 8, R, MAXV>(c, sa, ok, xv, v); break;
+          case (CAT_UNSIGNED << 4) | 4: p2_column<CAT_UNSIGNED, 4, R, MAXV>(c, sa, ok, xv, v); break;
+          case (CAT_UNSIGNED << 4) | 2: p2_column<CAT_UNSIGNED, 2, R, MAXV>(c, sa, ok, xv, v); break;
+          case (CAT_UNSIGNED << 4) | 1: p2_column<CAT_UNSIGNED, 1, R, MAXV>(c, sa, ok, xv, v); break;
+          default: p2_column<CAT_BOOL, 1, R, MAXV>(c, sa, ok, xv, v); break;
+        }
       }
     }
     __syncthreads();

@@ -139,6 +139,9 @@ typedef struct gb_tuning {
   int32_t force_mode;
   int64_t groups_hint;      /* caller's estimate of the number of groups (skips sampling) */
   int32_t profile;          /* 1: time the aggregation and compaction kernels with CUDA events */
+  int32_t scatter;          /* partitioned pass 1 launch shape, threads x rows per thread:
+                               0 512x8 (default), 1 256x16, 2 512x16, 3 1024x8, 4 512x8 with the
+                               next column's loads issued early, 5 1024x4, 6 256x8 */
 } gb_tuning;
 
 /* What the last gb_aggregate on a handle did. */

@@ -113,7 +113,7 @@ def test_three_keys_two_words():
     run_both([cb.Column.from_numpy(k) for k in ks], [(cb.Column.from_numpy(v), [agg.sum(), agg.variance(0)])])
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2])
 def test_all_ones_key_uses_special_slot(mode):
     cb, agg = _cb()
     n = 10_000
@@ -208,9 +208,10 @@ def test_config_shapes_medium(n, card, nulls):
               (cb.Column.from_numpy(v3, masks[2]), aggs)])
 
 
+@pytest.mark.parametrize("scatter", [0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("nulls", [False, True])
 @pytest.mark.parametrize("two_word", [False, True])
-def test_partitioned_mode(nulls, two_word):
+def test_partitioned_mode(nulls, two_word, scatter):
     cb, agg = _cb()
     rng = np.random.default_rng(31)
     n = 3_000_000
@@ -227,7 +228,7 @@ def test_partitioned_mode(nulls, two_word):
     aggs = [agg.sum(), agg.count(), agg.min(), agg.max(), agg.mean()]
     gb, *_ = run_both(keys, [(cb.Column.from_numpy(v1, ms[0]), aggs), (cb.Column.from_numpy(v2, ms[1]), aggs),
                              (cb.Column.from_numpy(v3, ms[2]), aggs + [agg.count(cb.NullPolicy.INCLUDE)])],
-                      include_null_keys=two_word, tuning={"force_mode": 2})
+                      include_null_keys=two_word, tuning={"force_mode": 2, "scatter": scatter})
     assert gb.stats()["mode"] == 2
 
 
@@ -241,7 +242,8 @@ def test_partitioned_mode_is_chosen_for_many_groups():
     assert gb.stats()["mode"] == 2
 
 
-def test_partitioned_spill_when_groups_underestimated():
+@pytest.mark.parametrize("scatter", [0, 1])
+def test_partitioned_spill_when_groups_underestimated(scatter):
     cb, agg = _cb()
     rng = np.random.default_rng(33)
     n = 1_500_000
@@ -251,7 +253,25 @@ def test_partitioned_spill_when_groups_underestimated():
     f = rng.random(n).astype(np.float32)
     run_both([cb.Column.from_numpy(key)], [(cb.Column.from_numpy(v), [agg.sum(), agg.count(), agg.min()]),
                                            (cb.Column.from_numpy(f, rng.random(n) > 0.2), [agg.mean(), agg.max()])],
-             tuning={"force_mode": 2, "groups_hint": 1000})
+             tuning={"force_mode": 2, "groups_hint": 1000, "scatter": scatter})
+
+
+@pytest.mark.parametrize("scatter", [0, 1])
+def test_partitioned_all_ones_key_heavy(scatter):
+    """40% of the rows carry the all-ones key: one partition aggregates them in
+    its dedicated shared slot, merged into the global table's slot at flush."""
+    cb, agg = _cb()
+    rng = np.random.default_rng(35)
+    n = 2_000_000
+    key = rng.integers(0, 200_000, n).astype(np.int64)
+    key[rng.random(n) < 0.4] = -1
+    v = rng.integers(-10**6, 10**6, n).astype(np.int64)
+    d = rng.normal(size=n)
+    gb, *_ = run_both([cb.Column.from_numpy(key)],
+                      [(cb.Column.from_numpy(v, rng.random(n) > 0.1), [agg.sum(), agg.count(), agg.min(), agg.max()]),
+                       (cb.Column.from_numpy(d, rng.random(n) > 0.1), [agg.mean(), agg.min(), agg.max()])],
+                      tuning={"force_mode": 2, "scatter": scatter})
+    assert gb.stats()["mode"] == 2
 
 
 def test_partitioned_skew_falls_back():
