@@ -3,12 +3,13 @@ drop-in for libcudf's ``cudf::groupby::groupby(keys, null_policy).aggregate``
 path.  The compute path is the CUDA library built by ``cudf_b200.build``; there
 is no CPU fallback."""
 from . import aggregation
-from .column import Column, Table
+from .column import Column, HostStaging, Table
 from .batch import BatchGroupBy
 from .groupby import GroupBy, GroupByRequest
 from .serving import Server
 from .types import Kind, NullPolicy, Sorted, TypeId
+from .frame import DataFrame
 
-__all__ = ["aggregation", "BatchGroupBy", "Column", "Table", "GroupBy", "GroupByRequest", "Kind", "NullPolicy",
-           "Server", "Sorted", "TypeId"]
+__all__ = ["aggregation", "BatchGroupBy", "Column", "DataFrame", "HostStaging", "Table", "GroupBy", "GroupByRequest",
+           "Kind", "NullPolicy", "Server", "Sorted", "TypeId"]
 __version__ = "0.1.0"

@@ -57,7 +57,7 @@ class Column:
 
     @staticmethod
     def from_numpy(arr, valid=None, type_id: Optional[int] = None, device="cuda") -> "Column":
-        arr = np.ascontiguousarray(arr)
+        arr = np.array(arr, copy=True, order="C") if not np.asarray(arr).flags.writeable else np.ascontiguousarray(arr)
         if type_id is None:
             type_id = {np.dtype(v): k for k, v in NUMPY_DTYPE.items()
                        if k not in (TypeId.BOOL8,) and k < 12}[arr.dtype]
@@ -127,6 +127,39 @@ class Table:
 
     def __len__(self):
         return len(self.columns)
+
+
+class HostStaging:
+    """Pinned host buffers reused across device->host copies of results.
+
+    A copy into pageable host memory (``tensor.cpu()``) runs at a few GB/s,
+    one into pinned memory at the PCIe rate (~55 GB/s on B200 hosts), so
+    callers that read results back every call keep one of these.  The arrays
+    ``to_host`` returns are views into the staging buffers: they stay valid
+    until the next ``to_host`` call on the same staging object."""
+
+    def __init__(self):
+        self._bufs: list = []
+
+    def to_host(self, tensors: Sequence[torch.Tensor], stream=None) -> list:
+        out = []
+        for i, t in enumerate(tensors):
+            nbytes = t.numel() * t.element_size()
+            if i >= len(self._bufs) or self._bufs[i].numel() < nbytes:
+                buf = torch.empty(max(nbytes, 1), dtype=torch.uint8).pin_memory()
+                if i >= len(self._bufs):
+                    self._bufs.append(buf)
+                else:
+                    self._bufs[i] = buf
+            view = self._bufs[i][:nbytes].view(t.dtype) if nbytes else torch.empty(0, dtype=t.dtype)
+            if nbytes:
+                view.copy_(t.reshape(-1), non_blocking=True)
+            out.append(view)
+        if stream is not None:
+            stream.synchronize()
+        else:
+            torch.cuda.current_stream().synchronize()
+        return [v.numpy() for v in out]
 
 
 class _CAI:
