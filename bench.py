@@ -94,14 +94,15 @@ def make_inputs_device(n: int, seed: int, device, key_seed=None):
 
 class ClockSampler:
     """SM clocks and throttle reasons during the timed region, read through NVML
-    (the library nvidia-smi uses) from a background thread every 250 ms.  An
+    (the library nvidia-smi uses) from a background thread every 50 ms.  An
     nvidia-smi subprocess polling the driver stalls CUDA API calls for tens of
-    milliseconds, which would show up in the timed region."""
+    milliseconds, which would show up in the timed region; in-process NVML
+    queries cost microseconds once each kind has been made once."""
 
     REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
                "sw_power_cap": 0x4}
 
-    def __init__(self, index: int, period: float = 0.25):
+    def __init__(self, index: int, period: float = 0.05):
         self.index = index
         self.period = period
         self.samples = []
@@ -123,6 +124,10 @@ class ClockSampler:
                     idx = self.index
             self.h = pynvml.nvmlDeviceGetHandleByIndex(idx)
             self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            # the first query of each kind costs milliseconds inside the
+            # driver: make them here, before the timed region starts
+            pynvml.nvmlDeviceGetClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            pynvml.nvmlDeviceGetCurrentClocksEventReasons(self.h)
             self.ok = True
             self.t = threading.Thread(target=self._run, daemon=True)
             self.t.start()

@@ -38,12 +38,57 @@ class Column:
                  size: Optional[int] = None, offset: int = 0, null_count: Optional[int] = None,
                  _owner=None):
         self.type_id = TypeId(type_id)
-        self.data = data
-        self.mask = mask
+        self._data = data
+        self._mask = mask
+        self._raw = None  # (data ptr, mask ptr) of an engine-owned result not yet wrapped
         self.offset = int(offset)
         self.size = int(data.numel() - self.offset if size is None else size)
         self._null_count = null_count
         self._owner = _owner
+
+    @staticmethod
+    def from_device_buffers(type_id: int, data_ptr: int, mask_ptr: int, size: int, null_count: int,
+                            owner) -> "Column":
+        """A zero-copy column over engine-owned device buffers.  The torch
+        views are made on first access, so results nobody reads cost no
+        wrapping; `owner` keeps the buffers alive."""
+        c = Column.__new__(Column)
+        c.type_id = TypeId(type_id)
+        c._data = None
+        c._mask = None
+        c._raw = (int(data_ptr or 0), int(mask_ptr or 0))
+        c.offset = 0
+        c.size = int(size)
+        c._null_count = int(null_count)
+        c._owner = owner
+        return c
+
+    def _materialize(self):
+        if self._raw is not None:
+            dp, mp = self._raw
+            self._raw = None
+            self._data = tensor_from_device(dp, self.size, self.type_id, self._owner)
+            self._mask = mask_from_device(mp, self.size, self._owner)
+
+    @property
+    def data(self) -> torch.Tensor:
+        self._materialize()
+        return self._data
+
+    @data.setter
+    def data(self, t: torch.Tensor):
+        self._raw = None
+        self._data = t
+
+    @property
+    def mask(self) -> Optional[torch.Tensor]:
+        self._materialize()
+        return self._mask
+
+    @mask.setter
+    def mask(self, m: Optional[torch.Tensor]):
+        self._materialize()
+        self._mask = m
 
     # -- construction ---------------------------------------------------
     @staticmethod
@@ -72,6 +117,9 @@ class Column:
 
     # -- views ----------------------------------------------------------
     def gb_view(self) -> _lib.GbColumn:
+        if self._raw is not None:
+            dp, mp = self._raw
+            return _lib.GbColumn(int(self.type_id), self.size, dp if self.size else 0, mp, 0)
         return _lib.GbColumn(int(self.type_id), self.size, self.data.data_ptr() if self.data.numel() else 0,
                              0 if self.mask is None else self.mask.data_ptr(), self.offset)
 

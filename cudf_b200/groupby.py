@@ -51,10 +51,8 @@ def _stream_handle(stream) -> int:
 
 
 def _out_column(oc: _lib.GbOutColumn, owner) -> Column:
-    n = int(oc.size)
-    data = tensor_from_device(oc.data or 0, n, oc.type_id, owner)
-    mask = mask_from_device(oc.null_mask or 0, n, owner)
-    return Column(oc.type_id, data, mask, size=n, null_count=int(oc.null_count), _owner=owner)
+    return Column.from_device_buffers(oc.type_id, oc.data or 0, oc.null_mask or 0, int(oc.size),
+                                      int(oc.null_count), owner)
 
 
 class GroupBy:
