@@ -579,6 +579,134 @@ def run_serve(args):
     return 0
 
 
+def _zipf_pairs(n, dev, g, s=1.1, support=50_000_000):
+    """Pair indices with P(p) proportional to (p+1)^-s on [0, support), by the
+    continuous inverse CDF of that power law (seeded torch generator)."""
+    import torch
+    u = torch.rand(n, device=dev, generator=g, dtype=torch.float64)
+    a = 1.0 - s
+    top = (support + 1.0) ** a
+    x = (1.0 - u * (1.0 - top)) ** (1.0 / a) - 1.0
+    return x.floor().clamp_(0, support - 1).to(torch.int64)
+
+
+def run_config(args):
+    """The other single-GPU shapes of the benchmark, one aggregate() per step:
+      zipf  -- 100M rows; (k1 int32, k2 int64) = divmod(p, 1000) with p Zipf(1.1)
+               on [0, 50M); 5% nulls in each key column, null keys included
+               (INCLUDE); v_int int64 uniform [0, 1e6], v_f f64 uniform [0, 1);
+               SUM, COUNT, MAX of each; seed 2.
+      small -- 1M rows; int32 key uniform over 1000 values; v1 int64 uniform
+               [0, 1e6], v2 f64 uniform [0, 1); v1 sum/count/min/max, v2 mean;
+               no nulls; seed 0.
+    Inputs are generated on the device; `value` is rows/s of the aggregate()
+    call; cpu_baseline runs the oracle on the same distributions."""
+    import torch
+    import cudf_b200 as cb
+    from cudf_b200 import aggregation as agg
+    from cudf_b200.column import pack_mask
+    from cudf_b200.types import NullPolicy, TypeId
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    g = torch.Generator(device=dev)
+    if args.workload == "zipf":
+        n = args.rows if args.rows != N_ROWS else 100_000_000
+        g.manual_seed(2)
+        p = _zipf_pairs(n, dev, g)
+        k1 = (p // 1000).to(torch.int32)
+        k2 = p % 1000
+        del p
+        km = [pack_mask(torch.rand(n, device=dev, generator=g) >= 0.05) for _ in range(2)]
+        vi = torch.randint(0, 10**6 + 1, (n,), device=dev, generator=g, dtype=torch.int64)
+        vf = torch.rand(n, device=dev, generator=g, dtype=torch.float64)
+        keys = cb.Table([cb.Column(TypeId.INT32, k1, km[0]), cb.Column(TypeId.INT64, k2, km[1])])
+        aggs = [agg.sum(), agg.count(), agg.max()]
+        reqs = [cb.GroupByRequest(cb.Column(TypeId.INT64, vi), aggs), cb.GroupByRequest(cb.Column(TypeId.FLOAT64, vf), aggs)]
+        policy = NullPolicy.INCLUDE
+        workload = ("groupby 100M rows, (int32, int64) keys = divmod(Zipf(1.1) on [0,50M), 1000), 5% key nulls, "
+                    "INCLUDE, int64 + f64 values, sum/count/max")
+        inp = n * (4 + 8 + 8 + 8) + 2 * ((n + 31) // 32) * 4
+    else:
+        n = args.rows if args.rows != N_ROWS else 1_000_000
+        g.manual_seed(0)
+        k = torch.randint(0, 1000, (n,), device=dev, generator=g, dtype=torch.int32)
+        v1 = torch.randint(0, 10**6 + 1, (n,), device=dev, generator=g, dtype=torch.int64)
+        v2 = torch.rand(n, device=dev, generator=g, dtype=torch.float64)
+        keys = cb.Table([cb.Column(TypeId.INT32, k)])
+        reqs = [cb.GroupByRequest(cb.Column(TypeId.INT64, v1), [agg.sum(), agg.count(), agg.min(), agg.max()]),
+                cb.GroupByRequest(cb.Column(TypeId.FLOAT64, v2), [agg.mean()])]
+        policy = NullPolicy.EXCLUDE
+        workload = "groupby 1M rows, int32 key over 1000 values, v1 int64 sum/count/min/max, v2 f64 mean"
+        inp = n * (4 + 8 + 8)
+    torch.cuda.synchronize()
+    gb = cb.GroupBy(keys, policy)
+    gb.set_profile(True)
+    for _ in range(args.warmup):
+        gb.aggregate(reqs)
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kms = []
+    with ClockSampler(0) as clk:
+        a.record(stream)
+        for _ in range(args.steps):
+            uk, res = gb.aggregate(reqs)
+            kms.append(gb.stats()["agg_kernel_ms"])
+        b.record(stream)
+        torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    st = gb.stats()
+    groups = uk.num_rows()
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    kmean = float(np.mean(kms))
+    line = {"metric": f"groupby rows/s ({args.workload})", "value": n / (ms * 1e-3), "unit": "rows/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/int64/f64",
+            "data": "synthetic", "config": {"workload": workload, "rows": n, "groups": groups},
+            "roofline": {"bound": "hbm", "achieved": inp / (kmean * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": inp / (kmean * 1e-3) / 1e9 / peak, "traffic": None,
+                         "kernel": KERNELS_BY_MODE.get(st["mode"]), "kernel_ms": kmean,
+                         "algorithmic_bytes": inp},
+            "engine": st, "clocks": clk.summary()}
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = _cpu_config(args.workload, min(n, args.cpu_sample))
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _cpu_config(workload, n):
+    """The oracle on n rows of the same distributions (numpy generator)."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(2 if workload == "zipf" else 0)
+    if workload == "zipf":
+        u = rng.random(n)
+        a = 1.0 - 1.1
+        p = np.clip(np.floor((1.0 - u * (1.0 - (50_000_001.0) ** a)) ** (1.0 / a) - 1.0), 0, 49_999_999).astype(np.int64)
+        keys = [O.HostColumn(O.INT32, (p // 1000).astype(np.int32), rng.random(n) >= 0.05),
+                O.HostColumn(O.INT64, p % 1000, rng.random(n) >= 0.05)]
+        kinds = [O.SUM, O.COUNT_VALID, O.MAX]
+        reqs = [(O.HostColumn(O.INT64, rng.integers(0, 10**6, n, endpoint=True)), kinds),
+                (O.HostColumn(O.FLOAT64, rng.random(n)), kinds)]
+        inc = True
+    else:
+        keys = [O.HostColumn(O.INT32, rng.integers(0, 1000, n).astype(np.int32))]
+        reqs = [(O.HostColumn(O.INT64, rng.integers(0, 10**6, n, endpoint=True)), [O.SUM, O.COUNT_VALID, O.MIN, O.MAX]),
+                (O.HostColumn(O.FLOAT64, rng.random(n)), [O.MEAN])]
+        inc = False
+    O.groupby(keys, reqs, include_null_keys=inc, nthreads=threads)
+    t = time.perf_counter()
+    O.groupby(keys, reqs, include_null_keys=inc, nthreads=threads)
+    v = n / (time.perf_counter() - t)
+    return {"value": v, "unit": "rows/s", "cores": threads, "kind": "port",
+            "sample": f"{n} rows with the workload's distributions through oracle/gb_oracle.c, {threads} threads"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -589,7 +717,7 @@ def main():
     ap.add_argument("--tuning", default="")
     ap.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE_ROWS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve"])
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "zipf", "small"])
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--duration", type=float, default=5.0)
@@ -600,6 +728,8 @@ def main():
         return run_batch(args)
     if args.workload == "serve" and args.impl == "engine":
         return run_serve(args)
+    if args.workload in ("zipf", "small") and args.impl == "engine":
+        return run_config(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_engine(args)

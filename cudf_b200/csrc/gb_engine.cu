@@ -445,6 +445,25 @@ uint32_t* pinned()
   return t_pinned;
 }
 
+// HyperLogLog cardinality from 2^kHllBits registers (Flajolet et al. 2007):
+// E = alpha_m m^2 / sum 2^-M[j], with linear counting m ln(m/V) while E is
+// below 2.5 m and V registers are still zero.  64-bit hashes need no
+// large-range correction.
+double hll_estimate(const std::vector<uint32_t>& regs)
+{
+  const double m = (double)regs.size();
+  double z = 0;
+  int zeros = 0;
+  for (uint32_t r : regs) {
+    z += std::ldexp(1.0, -(int)r);
+    zeros += r == 0;
+  }
+  const double alpha = 0.7213 / (1.0 + 1.079 / m);
+  double e = alpha * m * m / z;
+  if (e <= 2.5 * m && zeros > 0) e = m * std::log(m / zeros);
+  return e;
+}
+
 int grid_for(const void* kernel, int block, size_t smem, int bps_cap)
 {
   DevInfo d = dev_info();
@@ -519,44 +538,42 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   // ---- group-count estimate from a key sample ----
   int64_t est;
   std::vector<uint32_t> buckets;
+  bool exact_buckets = false;  // buckets hold exact row counts (full-pass sketch)
   int64_t nsamp = 0;
   if (opt.groups_hint >= 0) {
     est = std::max<int64_t>(1, opt.groups_hint);
   } else if (n <= 65536) {
     est = n;
   } else {
-    nsamp = std::min<int64_t>(n, 1 << 18);
-    uint64_t scap = next_pow2((uint64_t)(2 * nsamp));
-    size_t sbytes = (scap + 1) * 32;
-    uint8_t* ST = (uint8_t*)S.get(sbytes);
-    unsigned int* bk = (unsigned int*)S.get(sizeof(unsigned int) << kBucketBits);
-    ck(cudaMemsetAsync(bk, 0, sizeof(unsigned int) << kBucketBits, stream), "memset buckets");
-    SlotTemplate t;
-    std::memset(&t, 0, sizeof(t));
-    std::memset(&t, 0xFF, 16);
-    k_init_slots<<<dev.sms * 4, 256, 0, stream>>>(ST, (int64_t)scap + 1, 32, t);  // 16 B key | u32 count
-    TableRef SR{ST, scap - 1, 32, P.key_words, counters + 16};
-    k_sample<<<dev.sms * 4, 256, 0, stream>>>(P, SR, nsamp, bk);
-    k_sample_stats<<<dev.sms * 4, 256, 0, stream>>>(P, SR);
-    st.kernels += 3;
-    ck(cudaGetLastError(), "sample launch");
-    mark("sample launched");
-    buckets.resize((size_t)1 << kBucketBits);
-    ck(cudaMemcpyAsync(host, counters + 16, 16 * 4, cudaMemcpyDeviceToHost, stream), "sample d2h");
-    ck(cudaMemcpyAsync(buckets.data(), bk, buckets.size() * 4, cudaMemcpyDeviceToHost, stream), "bucket d2h");
-    ck(cudaStreamSynchronize(stream), "sample sync");
-    S.put(ST);
-    S.put(bk);
-    double d = host[4], f1 = host[5], f2 = host[6], m = host[3];
-    if (nsamp >= n) est = (int64_t)d;
-    else {
-      // bias-corrected Chao1 on the sample; scaled up when the sample saw
-      // mostly singletons (high cardinality)
-      double c1 = d + f1 * (f1 - 1) / (2 * (f2 + 1));
-      if (m > 0 && f1 > 0.9 * m) c1 = std::max(c1, d * (double)n / m);
-      est = (int64_t)std::min<double>((double)n, std::max(d, c1));
+    // full pass over the keys: exact rows per hash bucket (partition region
+    // sizes) and a HyperLogLog estimate of the number of distinct keys
+    unsigned int* hll = (unsigned int*)S.get((sizeof(unsigned int) << kHllBits) + (sizeof(unsigned int) << kBucketBits));
+    unsigned int* bk = hll + (1 << kHllBits);
+    ck(cudaMemsetAsync(hll, 0, (sizeof(unsigned int) << kHllBits) + (sizeof(unsigned int) << kBucketBits), stream),
+       "memset sketch");
+    {
+      const size_t sm = sketch_smem();
+      ck(cudaFuncSetAttribute(k_sketch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), "attr");
+      int grid = grid_for((const void*)k_sketch, 512, sm, 0);
+      grid = (int)std::min<int64_t>(grid, (n + 511) / 512);
+      k_sketch<<<grid, 512, sm, stream>>>(P, hll, bk);
     }
+    st.kernels += 1;
+    ck(cudaGetLastError(), "sketch launch");
+    mark("sketch launched");
+    std::vector<uint32_t> regs((size_t)1 << kHllBits);
+    buckets.resize((size_t)1 << kBucketBits);
+    ck(cudaMemcpyAsync(regs.data(), hll, regs.size() * 4, cudaMemcpyDeviceToHost, stream), "sketch d2h");
+    ck(cudaMemcpyAsync(buckets.data(), bk, buckets.size() * 4, cudaMemcpyDeviceToHost, stream), "sketch d2h");
+    ck(cudaStreamSynchronize(stream), "sketch sync");
+    S.put(hll);
+    exact_buckets = true;
+    int64_t valid_rows = 0;
+    for (auto b : buckets) valid_rows += b;
+    est = (int64_t)std::llround(hll_estimate(regs));
+    est = std::min<int64_t>(std::max<int64_t>(est, valid_rows > 0 ? 1 : 0), valid_rows);
     est = std::max<int64_t>(est, 1);
+    nsamp = valid_rows;
   }
   st.est_groups = est;
   mark("estimate");
@@ -574,7 +591,9 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   int scap = smem_cap_for(opt.smem_bytes);
   int sfill = std::max(1, (int)(scap * opt.smem_fill));
   int64_t smem_max = opt.smem_max_groups >= 0 ? opt.smem_max_groups : 2 * (int64_t)sfill;
-  const int scap2 = smem_cap_for(200 * 1024);
+  // partitioned pass 2: as many slots as fit ~220 KB (any count), one more
+  // for the all-ones key
+  const int scap2 = std::max(0, std::min(220 * 1024, dev.smem_optin - 8192) / P.slot_bytes - 1);
   const int sfill2 = std::max(1, (int)(scap2 * 0.8));
   bool part_ok = !P.has_arg && !P.need_second_pass && P.num_vals <= 8 && scap2 >= 256;
   for (int v = 0; v < P.num_vals; ++v) part_ok = part_ok && P.vals[v].basic;
@@ -595,34 +614,45 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   if (mode == 1 && scap < 16) mode = 0;
   if (mode == 2 && !part_ok) mode = 0;
 
-  // region sizes of the partitioned path from the sample's bucket counts
-  std::vector<int64_t> pbase, pend;
+  // region sizes of the partitioned path: exact rows per partition from the
+  // full-pass sketch (else the sample's share with slack)
+  std::vector<int64_t> pbase, pend, prows;
   if (mode == 2) {
-    if (buckets.empty()) {  // no sample (hint given or small input): uniform regions
+    if (buckets.empty()) {  // no sketch (hint given or small input): uniform regions
       buckets.assign((size_t)1 << kBucketBits, 1);
       nsamp = (int64_t)buckets.size();
+      exact_buckets = false;
     }
     int lg = 0;
     while ((1 << lg) < nparts) ++lg;
     int per_bucket = kBucketBits - lg;
     pbase.resize(nparts);
     pend.resize(nparts);
+    prows.resize(nparts);
     int64_t total = 0, maxload = 0;
     double samp = 0;
     for (auto b : buckets) samp += b;
     for (int p = 0; p < nparts; ++p) {
       double c = 0;
       for (int b = p << per_bucket; b < ((p + 1) << per_bucket); ++b) c += buckets[b];
-      int64_t expect = (int64_t)std::ceil((double)n * c / std::max(1.0, samp));
-      int64_t capp = std::max<int64_t>((int64_t)(1.3 * expect), (int64_t)(1.15 * n / nparts)) + 2048;
-      capp = std::min<int64_t>(capp, n);
+      int64_t capp;
+      if (exact_buckets) {
+        capp = (int64_t)c;
+        prows[p] = capp;
+      } else {
+        int64_t expect = (int64_t)std::ceil((double)n * c / std::max(1.0, samp));
+        capp = std::max<int64_t>((int64_t)(1.3 * expect), (int64_t)(1.15 * n / nparts)) + 2048;
+        capp = std::min<int64_t>(capp, n);
+        prows[p] = expect;
+        maxload = std::max<int64_t>(maxload, expect);
+      }
       pbase[p] = total;
       total += (capp + 31) & ~31ll;
       pend[p] = total;
-      maxload = std::max<int64_t>(maxload, expect);
     }
-    // heavy skew: one partition would hold far more than its share
-    if (opt.force_mode != 2 && maxload > 4 * (n / nparts) + 4096) mode = (scap >= 64) ? 1 : 0;
+    // heavy skew seen only through a sample: one partition could hold far
+    // more than its share (exact counts split heavy partitions instead)
+    if (!exact_buckets && opt.force_mode != 2 && maxload > 4 * (n / nparts) + 4096) mode = (scap >= 64) ? 1 : 0;
   }
   st.mode = mode;
 
@@ -696,8 +726,39 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       P2.vals[v].bits = A.bits;
       P2.vals[v].bit = v;
     }
-    uint64_t spill_cap = 1 << 16;
-    uint32_t spill_list = 1u << 18;
+    // pass-2 work: one item per partition, except that a partition holding
+    // far more rows than the average (a heavy key) is cut into row ranges
+    // handled by several CTAs, each merging its table into the global table
+    std::vector<PartItem> items;
+    int64_t nsplit = 0;
+    {
+      int64_t nrows = 0;
+      for (auto r : prows) nrows += r;
+      const int64_t chunk = std::max<int64_t>(nrows / std::max(1, nparts), 32768);
+      for (int p = 0; p < nparts; ++p) {
+        const int64_t r = prows[p];
+        if (exact_buckets && r > 2 * chunk) {
+          ++nsplit;
+          for (int64_t b = 0; b < r; b += chunk)
+            items.push_back(PartItem{p, 1, pbase[p] + b, pbase[p] + std::min(r, b + chunk)});
+        }
+      }
+      for (int p = 0; p < nparts; ++p) {
+        const int64_t r = prows[p];
+        if (!(exact_buckets && r > 2 * chunk)) items.push_back(PartItem{p, 0, pbase[p], pend[p]});
+      }
+    }
+    PartItem* d_items = (PartItem*)S.get(sizeof(PartItem) * items.size());
+    ck(cudaMemcpyAsync(d_items, items.data(), sizeof(PartItem) * items.size(), cudaMemcpyHostToDevice, stream), "h2d");
+    int nmerge = 0;
+    while (nmerge < (int)items.size() && items[nmerge].merge) ++nmerge;
+    // groups expected to miss their partition's shared table, plus those of
+    // split partitions, go to the global spill table
+    const double expect_spill = std::max(0.0, (double)est - 0.85 * (double)nparts * sfill2);
+    uint64_t spill_cap = next_pow2((uint64_t)std::max<double>(65536.0, 2.0 * expect_spill + 2.0 * (double)nsplit * scap2));
+    // spill list: room for the rows of the groups expected to spill
+    uint32_t spill_list = (uint32_t)std::min<uint64_t>(
+      1ull << 31, next_pow2((uint64_t)std::max<double>(262144.0, 4.0 * expect_spill)));
     int64_t dcap = (int64_t)(est * 1.5) + (int64_t)nparts * 256 + 4096;
     for (int attempt = 0;; ++attempt) {
       T = (uint8_t*)S.get((size_t)(spill_cap + 1) * P.slot_bytes);
@@ -706,28 +767,52 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       A.spill_cap = spill_list;
       k_init_slots<<<dev.sms * 4, 256, 0, stream>>>(T, (int64_t)spill_cap + 1, P.slot_bytes, tmpl);
       ck(cudaMemsetAsync(counters, 0, 16, stream), "memset");
-      // [6] dense overflow, [8] work, [10..11] dense count, [12] spill list length, [13] list overflow
+      // [6] dense overflow, [8..9] work, [10..11] dense count, [12] spill list length, [13] list overflow
       ck(cudaMemsetAsync(counters + 6, 0, 8 * 4, stream), "memset");
       G = TableRef{T, spill_cap - 1, P.slot_bytes, P.key_words, counters};
       DenseRef D{dense, dcap, (unsigned long long*)(counters + 10), counters + 6};
       // shared table plus the all-ones key's slot
       size_t sm2 = (size_t)(scap2 + 1) * P.slot_bytes;
-      auto launch2 = [&](auto kern, int nt) {
+      // items of split (heavy) partitions first, with rows of one slot
+      // combined per warp before their shared update; then the rest
+      auto launch2 = [&](auto kern, int nt, int first, int count, unsigned int* work) {
+        if (count <= 0) return;
+        PartArgs Ai = A;
+        Ai.items = d_items + first;
+        Ai.nitems = count;
+        Ai.work = work;
         ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2), "attr");
         int grid = grid_for((const void*)kern, nt, sm2, 0);
-        grid = std::min(grid, nparts);
-        kern<<<grid, nt, sm2, stream>>>(P2, A, G, D, scap2, sfill2, tmpl);
+        grid = std::min(grid, count);
+        kern<<<grid, nt, sm2, stream>>>(P2, Ai, G, D, scap2, sfill2, tmpl);
+        ++st.kernels;
       };
       const bool few = P.num_vals <= 4;
-      if (P.key_words == 1) few ? launch2(k_part_aggregate<1, 1, 1024, 4>, 1024) : launch2(k_part_aggregate<1, 1, 1024, 8>, 1024);
-      else few ? launch2(k_part_aggregate<2, 1, 1024, 4>, 1024) : launch2(k_part_aggregate<2, 1, 1024, 8>, 1024);
+      const int nrest = (int)items.size() - nmerge;
+      if (P.key_words == 1) {
+        if (few) {
+          launch2(k_part_aggregate<1, 1, 1024, 4, true>, 1024, 0, nmerge, counters + 8);
+          launch2(k_part_aggregate<1, 1, 1024, 4, false>, 1024, nmerge, nrest, counters + 9);
+        } else {
+          launch2(k_part_aggregate<1, 1, 1024, 8, true>, 1024, 0, nmerge, counters + 8);
+          launch2(k_part_aggregate<1, 1, 1024, 8, false>, 1024, nmerge, nrest, counters + 9);
+        }
+      } else {
+        if (few) {
+          launch2(k_part_aggregate<2, 1, 1024, 4, true>, 1024, 0, nmerge, counters + 8);
+          launch2(k_part_aggregate<2, 1, 1024, 4, false>, 1024, nmerge, nrest, counters + 9);
+        } else {
+          launch2(k_part_aggregate<2, 1, 1024, 8, true>, 1024, 0, nmerge, counters + 8);
+          launch2(k_part_aggregate<2, 1, 1024, 8, false>, 1024, nmerge, nrest, counters + 9);
+        }
+      }
       if (opt.profile) ck(cudaEventRecord(events()[1], stream), "event");
       // rows listed as not fitting their partition's table (none when the
       // sample sized the partitions well): one grid-stride launch that reads
       // the list length on the device
       k_part_spill<<<dev.sms * 2, 256, 0, stream>>>(P2, G, A);
       k_finish_count<<<1, 1, 0, stream>>>(P, G);
-      st.kernels += 4;
+      st.kernels += 3;
       ck(cudaGetLastError(), "partition aggregate launch");
       ck(cudaMemcpyAsync(host, counters, 64, cudaMemcpyDeviceToHost, stream), "d2h");
       ck(cudaStreamSynchronize(stream), "partition sync");

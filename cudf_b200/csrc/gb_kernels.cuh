@@ -419,6 +419,57 @@ static __global__ void __launch_bounds__(256) k_sample(const __grid_constant__ P
   }
 }
 
+// Full-pass key sketch: per hash bucket (top kBucketBits bits) the exact
+// number of rows with a valid key, and a HyperLogLog register array
+// (Flajolet, Fusy, Gandouet, Meunier 2007) of 2^kHllBits registers over the
+// same hashes: register index from hash bits 40-51, rank = position of the
+// first set bit among bits 39..0.  Each CTA builds both in shared memory and
+// merges them into `hll` (atomic max) and `buckets` (atomic add) at the end.
+constexpr int kHllBits = 12;
+inline size_t sketch_smem() { return ((size_t(1) << kHllBits) + (size_t(1) << kBucketBits)) * 4; }
+
+static __global__ void __launch_bounds__(512) k_sketch(const __grid_constant__ Plan P, unsigned int* hll,
+                                                       unsigned int* buckets)
+{
+  extern __shared__ unsigned int sk[];
+  unsigned int* reg = sk;
+  unsigned int* bk = sk + (1 << kHllBits);
+  for (int i = threadIdx.x; i < (1 << kHllBits) + (1 << kBucketBits); i += blockDim.x) sk[i] = 0;
+  __syncthreads();
+  const int64_t n = P.num_rows;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  auto add = [&](uint64_t h) {
+    atomicAdd(&bk[h >> (64 - kBucketBits)], 1u);
+    const uint64_t low = h << 24;
+    const unsigned rank = low ? (unsigned)__clzll((long long)low) + 1u : 41u;
+    atomicMax(&reg[(h >> 40) & ((1u << kHllBits) - 1)], rank);
+  };
+  if (P.num_keys == 1 && !P.keys[0].mask && P.keys[0].width == 8 && P.keys[0].cat != CAT_F64) {
+    // one plain 64-bit key: four rows per thread in flight
+    const unsigned long long* kd = (const unsigned long long*)P.keys[0].data + P.keys[0].offset;
+    int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (; row + 3 * stride < n; row += 4 * stride) {
+      uint64_t k[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) k[j] = __ldg(kd + row + j * stride);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) add(fmix64(k[j]));
+    }
+    for (; row < n; row += stride) add(fmix64(__ldg(kd + row)));
+  } else {
+    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n; row += stride) {
+      uint64_t w0, w1;
+      if (!pack_key(P, row, w0, w1)) continue;
+      add(hash_key(w0, w1, P.key_words));
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < (1 << kHllBits); i += blockDim.x)
+    if (reg[i]) atomicMax(hll + i, reg[i]);
+  for (int i = threadIdx.x; i < (1 << kBucketBits); i += blockDim.x)
+    if (bk[i]) atomicAdd(buckets + i, bk[i]);
+}
+
 // counters: [4] distinct, [5] seen once, [6] seen twice
 static __global__ void __launch_bounds__(256) k_sample_stats(const __grid_constant__ Plan P, TableRef S)
 {

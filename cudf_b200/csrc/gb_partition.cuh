@@ -20,6 +20,15 @@
 
 namespace gb {
 
+// One unit of pass-2 work: rows [begin, end) of partition `part`'s region.
+// `merge` = 1 when the partition is split over several items, whose tables
+// then all go to the global table.
+struct PartItem {
+  int32_t part;
+  int32_t merge;
+  int64_t begin, end;
+};
+
 struct PartArgs {
   int32_t nparts;
   int32_t shift;                 // partition = hash >> shift
@@ -33,6 +42,9 @@ struct PartArgs {
                                  // [12] spill list length, [13] spill list overflow
   int64_t* spill_rows;           // pass 2: rows that did not fit their shared table
   unsigned int spill_cap;
+  const PartItem* items;         // pass 2 work list
+  int32_t nitems;
+  unsigned int* work;            // pass 2 claim counter of this item list
 };
 
 struct DenseRef {
@@ -273,15 +285,18 @@ inline size_t part_scatter_smem(int kw, int tile, int nparts)
 
 // Shared-memory find-or-insert (bounded probes); null when the key does not
 // fit (table at its fill limit or too many probes) or is the all-ones key.
-__device__ __forceinline__ uint8_t* smem_slot(uint8_t* smem, int stride, uint64_t smask, int sfill,
+// The table has `scap` slots, any count: the start slot is the low 32 hash
+// bits scaled to [0, scap) (multiply-shift), so the table can fill all the
+// shared memory a CTA has instead of the largest power of two below it.
+__device__ __forceinline__ uint8_t* smem_slot(uint8_t* smem, int stride, uint32_t scap, int sfill,
                                               unsigned int* s_used, int words, uint64_t w0,
                                               uint64_t w1, uint64_t h)
 {
-  uint64_t i = h & smask;
+  uint32_t i = (uint32_t)(((uint64_t)(uint32_t)h * scap) >> 32);
   if (words == 1) {
     if (w0 == kEmpty) return nullptr;
     for (int p = 0; p < 64; ++p) {
-      unsigned long long* kp = (unsigned long long*)(smem + i * stride);
+      unsigned long long* kp = (unsigned long long*)(smem + (size_t)i * stride);
       uint64_t cur = *(volatile unsigned long long*)kp;
       if (cur == w0) return (uint8_t*)kp;
       if (cur == kEmpty) {
@@ -290,14 +305,14 @@ __device__ __forceinline__ uint8_t* smem_slot(uint8_t* smem, int stride, uint64_
         if (old == kEmpty) { atomicAdd(s_used, 1u); return (uint8_t*)kp; }
         if (old == w0) return (uint8_t*)kp;
       }
-      i = (i + 1) & smask;
+      i = i + 1 == scap ? 0 : i + 1;
     }
     return nullptr;
   }
   unsigned __int128 want = ((unsigned __int128)w1 << 64) | w0;
   const unsigned __int128 empty = ~(unsigned __int128)0;
   for (int p = 0; p < 64; ++p) {
-    unsigned __int128* kp = (unsigned __int128*)(smem + i * stride);
+    unsigned __int128* kp = (unsigned __int128*)(smem + (size_t)i * stride);
     ulonglong2 cur = vload2(kp);
     if (cur.x == w0 && cur.y == w1 && w0 != kEmpty) return (uint8_t*)kp;
     if ((cur.y >> 63) || cur.x == kEmpty) {
@@ -306,7 +321,7 @@ __device__ __forceinline__ uint8_t* smem_slot(uint8_t* smem, int stride, uint64_
       if (old == empty) { atomicAdd(s_used, 1u); return (uint8_t*)kp; }
       if (old == want) return (uint8_t*)kp;
     }
-    i = (i + 1) & smask;
+    i = i + 1 == scap ? 0 : i + 1;
   }
   return nullptr;
 }
@@ -363,16 +378,16 @@ static __global__ void __launch_bounds__(256) k_part_spill(const __grid_constant
 }
 
 // ---- pass 2 ----
-// Per-partition prologue: claim a partition, reset the shared table (`scap`
+// Per-item prologue: claim a work item, reset the shared table (`scap`
 // slots plus, for one-word keys, the slot of the all-ones key).  Returns the
-// partition id (>= nparts: no work left).
+// item index (>= nitems: no work left).
 template <int NT>
 __device__ __forceinline__ int p2_claim(const PartArgs& A, uint8_t* smem, int scap, int nw,
                                         const SlotTemplate& tmpl, int* s_part, unsigned int* s_used,
                                         unsigned int* s_spill)
 {
   if (threadIdx.x == 0) {
-    *s_part = (int)atomicAdd(A.counters + 8, 1u);
+    *s_part = (int)atomicAdd(A.work, 1u);
     *s_used = 0;
     *s_spill = 0;
   }
@@ -429,14 +444,41 @@ __device__ __forceinline__ void p2_flush(const Plan& P2, const TableRef& G, cons
   }
 }
 
+// Combines `v` over the lanes of `grp` (lanes sharing one slot); the result
+// is meaningful at the group's lowest lane.  A whole-warp group (one hot key)
+// folds in five butterfly steps, other groups through one shuffle per member.
+template <typename T, typename F>
+__device__ __forceinline__ T grp_reduce(unsigned grp, T v, F op)
+{
+  if (grp == 0xFFFFFFFFu) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+    return v;
+  }
+  unsigned rest = grp & (grp - 1);
+  T acc = v;
+  while (rest) {
+    const int src = __ffs(rest) - 1;
+    rest &= rest - 1;
+    acc = op(acc, __shfl_sync(grp, v, src));
+  }
+  return acc;
+}
+
 // One value column of a chunk of R rows per thread (values already loaded),
 // with the column's type fixed at compile time: each accumulator present
 // (sum, min, max, sum of squares) is one shared-memory reduction per row.
 // `ok` = 0 marks rows that are absent, null in this column, or were listed
 // as spills.
-template <int CAT, int W, int R, int MAXV>
+// With WAGG, lanes whose rows hit the same slot (`peers`, from one match per
+// row) first combine their values in registers and the group's lowest lane
+// makes the single shared update: rows of one hot key no longer queue on one
+// shared address (64-bit and floating-point shared reductions are
+// compare-and-swap loops on this architecture, which such contention makes
+// retry up to 32 times).
+template <int CAT, int W, int R, int MAXV, bool WAGG>
 __device__ __forceinline__ void p2_column(const ValCol& c, const uint32_t (&sa)[R], const uint32_t (&ok)[R],
-                                          const uint64_t (&xv)[R][MAXV], int v)
+                                          const uint64_t (&xv)[R][MAXV], int v, const unsigned (&peers)[R])
 {
   uint64_t x[R];
 #pragma unroll
@@ -448,9 +490,67 @@ __device__ __forceinline__ void p2_column(const ValCol& c, const uint32_t (&sa)[
   }
   const int so = c.sum_off, mo = c.min_off, xo = c.max_off, qo = c.sq_off;
   const bool sum32 = c.sum_op == OP_SUM_I32;
+  bool grouped[R];
+#pragma unroll
+  for (int j = 0; j < R; ++j) grouped[j] = false;
+  if (WAGG) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const unsigned grp = peers[j] & __ballot_sync(0xFFFFFFFFu, ok[j] != 0);
+      if (!ok[j] || __popc(grp) == 1) continue;  // singles take the plain path below
+      grouped[j] = true;
+      const bool lead = lane == __ffs(grp) - 1;
+      const uint32_t a = sa[j];
+      auto add64 = [](uint64_t p, uint64_t q) { return p + q; };
+      auto min64 = [](uint64_t p, uint64_t q) { return p < q ? p : q; };
+      auto max64 = [](uint64_t p, uint64_t q) { return p > q ? p : q; };
+      auto min32 = [](uint32_t p, uint32_t q) { return p < q ? p : q; };
+      auto max32 = [](uint32_t p, uint32_t q) { return p > q ? p : q; };
+      if (CAT == CAT_F64) {
+        const double d = __longlong_as_double((long long)x[j]);
+        if (so >= 0) { const double t = grp_reduce(grp, d, [](double p, double q) { return p + q; }); if (lead) sred_add_f64(a + so, t); }
+        if (mo >= 0) { const uint64_t t = grp_reduce(grp, ord64_f(d, true), min64); if (lead) sred_min_u64(a + mo, t); }
+        if (xo >= 0) { const uint64_t t = grp_reduce(grp, ord64_f(d, false), max64); if (lead) sred_max_u64(a + xo, t); }
+        if (qo >= 0) { const double t = grp_reduce(grp, d * d, [](double p, double q) { return p + q; }); if (lead) sred_add_f64(a + qo, t); }
+      } else if (CAT == CAT_F32) {
+        const float f = __uint_as_float((uint32_t)x[j]);
+        if (so >= 0) { const float t = grp_reduce(grp, f, [](float p, float q) { return p + q; }); if (lead) sred_add_f32(a + so, t); }
+        if (mo >= 0) { const uint32_t t = grp_reduce(grp, ord32_f(f, true), min32); if (lead) sred_min_u32(a + mo, t); }
+        if (xo >= 0) { const uint32_t t = grp_reduce(grp, ord32_f(f, false), max32); if (lead) sred_max_u32(a + xo, t); }
+        if (qo >= 0) { const float t = grp_reduce(grp, f * f, [](float p, float q) { return p + q; }); if (lead) sred_add_f32(a + qo, t); }
+      } else {
+        int64_t iv;
+        if (CAT == CAT_SIGNED) iv = W == 8 ? (int64_t)x[j] : W == 4 ? (int64_t)(int32_t)x[j]
+                                          : W == 2 ? (int64_t)(int16_t)x[j] : (int64_t)(int8_t)x[j];
+        else if (CAT == CAT_BOOL) iv = x[j] != 0;
+        else iv = (int64_t)x[j];
+        if (so >= 0) {
+          const uint64_t t = grp_reduce(grp, (uint64_t)iv, add64);  // wrapping, as the atomics
+          if (lead) {
+            if (sum32) sred_add_u32(a + so, (uint32_t)t);
+            else sred_add_u64(a + so, t);
+          }
+        }
+        if (W == 8) {
+          const uint64_t o = CAT == CAT_SIGNED ? ((uint64_t)iv ^ 0x8000000000000000ull) : (uint64_t)iv;
+          if (mo >= 0) { const uint64_t t = grp_reduce(grp, o, min64); if (lead) sred_min_u64(a + mo, t); }
+          if (xo >= 0) { const uint64_t t = grp_reduce(grp, o, max64); if (lead) sred_max_u64(a + xo, t); }
+        } else {
+          const uint32_t o = CAT == CAT_SIGNED ? ((uint32_t)(int32_t)iv ^ 0x80000000u) : (uint32_t)iv;
+          if (mo >= 0) { const uint32_t t = grp_reduce(grp, o, min32); if (lead) sred_min_u32(a + mo, t); }
+          if (xo >= 0) { const uint32_t t = grp_reduce(grp, o, max32); if (lead) sred_max_u32(a + xo, t); }
+        }
+        if (qo >= 0) {
+          const uint64_t t = grp_reduce(grp, (uint64_t)iv * (uint64_t)iv, add64);
+          if (lead) sred_add_u64(a + qo, t);
+        }
+      }
+    }
+  }
 #pragma unroll
   for (int j = 0; j < R; ++j) {
-    if (!ok[j]) continue;
+    if (!ok[j] || grouped[j]) continue;
     const uint32_t a = sa[j];
     if (CAT == CAT_F64) {
       const double d = __longlong_as_double((long long)x[j]);
@@ -499,7 +599,7 @@ __device__ __forceinline__ void p2_column(const ValCol& c, const uint32_t (&sa)[
 // 128-byte line of the key, value and validity arrays), then the columns are
 // applied one at a time, each through code specialised for its type, so the
 // per-type dispatch happens once per column and chunk instead of per row.
-template <int KW, int R, int NT, int MAXV>
+template <int KW, int R, int NT, int MAXV, bool WAGG>
 __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant__ Plan P2,
                                                           const __grid_constant__ PartArgs A,
                                                           TableRef G, DenseRef D, int scap, int sfill,
@@ -514,7 +614,6 @@ __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant_
   if (threadIdx.x == 0) s_new = 0;
   const int stride = G.stride;
   const int nw = stride / 8;
-  const uint64_t smask = (uint64_t)scap - 1;
   const bool have_bits = A.bits != nullptr;
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
   const int nv = P2.num_vals;
@@ -538,10 +637,11 @@ __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant_
     if (have_bits) take(A.bits, 1);
   }
   for (;;) {
-    const int p = p2_claim<NT>(A, smem, scap + (KW == 1), nw, tmpl, &s_part, &s_used, &s_spill);
-    if (p >= A.nparts) break;
-    const int64_t b = A.base[p];
-    const int64_t e = min((int64_t)A.cursor[p], A.end[p]);
+    const int it = p2_claim<NT>(A, smem, scap + (KW == 1), nw, tmpl, &s_part, &s_used, &s_spill);
+    if (it >= A.nitems) break;
+    const PartItem item = A.items[it];
+    const int64_t b = item.begin;
+    const int64_t e = min(item.end, min((int64_t)A.cursor[item.part], A.end[item.part]));
     auto load_keys = [&](int64_t r0, uint64_t (&k0)[R], uint64_t (&k1)[R], uint32_t (&vb)[R]) {
 #pragma unroll
       for (int j = 0; j < R; ++j) {
@@ -580,16 +680,32 @@ __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant_
         const uint64_t h = hash_key(k0[j], k1[j], KW);
         uint8_t* slot = (KW == 1 && k0[j] == kEmpty)
                           ? smem + (size_t)scap * stride
-                          : smem_slot(smem, stride, smask, sfill, &s_used, KW, k0[j], k1[j], h);
+                          : smem_slot(smem, stride, (uint32_t)scap, sfill, &s_used, KW, k0[j], k1[j], h);
         if (slot == nullptr) {
+          // listed for the global table; one list reservation per warp
           s_spill = 1;
-          const unsigned at = atomicAdd(A.counters + 12, 1u);
+          const unsigned mates = __activemask();
+          const int leader = __ffs(mates) - 1;
+          const int lane = threadIdx.x & 31;
+          unsigned at = 0;
+          if (lane == leader) at = atomicAdd(A.counters + 12, (unsigned)__popc(mates));
+          at = __shfl_sync(mates, at, leader) + __popc(mates & ((1u << lane) - 1));
           if (at < A.spill_cap) A.spill_rows[at] = row[j];
           else atomicOr(A.counters + 13, 1u);
           continue;
         }
         sa[j] = sbase + (uint32_t)(slot - smem);
-        sred_add_u32(sa[j] + P2.rows_off, 1u);
+      }
+      // lanes sharing a slot (WAGG): one match per row; rows counted by the
+      // group's lowest lane
+      unsigned peers[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        peers[j] = 1u << (threadIdx.x & 31);
+        if (WAGG) peers[j] = __match_any_sync(0xFFFFFFFFu, sa[j] ? sa[j] : (0x80000000u | (threadIdx.x & 31)));
+        if (!sa[j]) continue;
+        if (!WAGG) sred_add_u32(sa[j] + P2.rows_off, 1u);
+        else if ((threadIdx.x & 31) == __ffs(peers[j]) - 1) sred_add_u32(sa[j] + P2.rows_off, __popc(peers[j]));
       }
       uint32_t cur_vb[R];
 #pragma unroll
@@ -615,25 +731,31 @@ __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant_
         for (int j = 0; j < R; ++j) {
           const bool valid = (cur_vb[j] >> v) & 1;
           ok[j] = sa[j] != 0 && valid;
-          if (sa[j] != 0 && !valid && c.nulls_off >= 0) sred_add_u32(sa[j] + c.nulls_off, 1u);
+          if (WAGG) {
+            const unsigned ng = peers[j] & __ballot_sync(0xFFFFFFFFu, sa[j] != 0 && !valid);
+            if (sa[j] != 0 && !valid && c.nulls_off >= 0 && (threadIdx.x & 31) == __ffs(ng) - 1)
+              sred_add_u32(sa[j] + c.nulls_off, __popc(ng));
+          } else if (sa[j] != 0 && !valid && c.nulls_off >= 0) {
+            sred_add_u32(sa[j] + c.nulls_off, 1u);
+          }
         }
         switch ((c.cat << 4) | c.width) {
-          case (CAT_F64 << 4) | 8: p2_column<CAT_F64, 8, R, MAXV>(c, sa, ok, xv, v); break;
-          case (CAT_F32 << 4) | 4: p2_column<CAT_F32, 4, R, MAXV>(c, sa, ok, xv, v); break;
-          case (CAT_SIGNED << 4) | 8: p2_column<CAT_SIGNED, 8, R, MAXV>(c, sa, ok, xv, v); break;
-          case (CAT_SIGNED << 4) | 4: p2_column<CAT_SIGNED, 4, R, MAXV>(c, sa, ok, xv, v); break;
-          case (CAT_SIGNED << 4) | 2: p2_column<CAT_SIGNED, 2, R, MAXV>(c, sa, ok, xv, v); break;
-          case (CAT_SIGNED << 4) | 1: p2_column<CAT_SIGNED, 1, R, MAXV>(c, sa, ok, xv, v); break;
-          case (CAT_UNSIGNED << 4) | 8: p2_column<CAT_UNSIGNED, 8, R, MAXV>(c, sa, ok, xv, v); break;
-          case (CAT_UNSIGNED << 4) | 4: p2_column<CAT_UNSIGNED, 4, R, MAXV>(c, sa, ok, xv, v); break;
-          case (CAT_UNSIGNED << 4) | 2: p2_column<CAT_UNSIGNED, 2, R, MAXV>(c, sa, ok, xv, v); break;
-          case (CAT_UNSIGNED << 4) | 1: p2_column<CAT_UNSIGNED, 1, R, MAXV>(c, sa, ok, xv, v); break;
-          default: p2_column<CAT_BOOL, 1, R, MAXV>(c, sa, ok, xv, v); break;
+          case (CAT_F64 << 4) | 8: p2_column<CAT_F64, 8, R, MAXV, WAGG>(c, sa, ok, xv, v, peers); break;
+          case (CAT_F32 << 4) | 4: p2_column<CAT_F32, 4, R, MAXV, WAGG>(c, sa, ok, xv, v, peers); break;
+          case (CAT_SIGNED << 4) | 8: p2_column<CAT_SIGNED, 8, R, MAXV, WAGG>(c, sa, ok, xv, v, peers); break;
+          case (CAT_SIGNED << 4) | 4: p2_column<CAT_SIGNED, 4, R, MAXV, WAGG>(c, sa, ok, xv, v, peers); break;
+          case (CAT_SIGNED << 4) | 2: p2_column<CAT_SIGNED, 2, R, MAXV, WAGG>(c, sa, ok, xv, v, peers); break;
+          case (CAT_SIGNED << 4) | 1: p2_column<CAT_SIGNED, 1, R, MAXV, WAGG>(c, sa, ok, xv, v, peers); break;
+          case (CAT_UNSIGNED << 4) | 8: p2_column<CAT_UNSIGNED, 8, R, MAXV, WAGG>(c, sa, ok, xv, v, peers); break;
+          case (CAT_UNSIGNED << 4) | 4: p2_column<CAT_UNSIGNED, 4, R, MAXV, WAGG>(c, sa, ok, xv, v, peers); break;
+          case (CAT_UNSIGNED << 4) | 2: p2_column<CAT_UNSIGNED, 2, R, MAXV, WAGG>(c, sa, ok, xv, v, peers); break;
+          case (CAT_UNSIGNED << 4) | 1: p2_column<CAT_UNSIGNED, 1, R, MAXV, WAGG>(c, sa, ok, xv, v, peers); break;
+          default: p2_column<CAT_BOOL, 1, R, MAXV, WAGG>(c, sa, ok, xv, v, peers); break;
         }
       }
     }
     __syncthreads();
-    p2_flush<NT, ScanT>(P2, G, D, smem, scap, s_spill != 0, scan_tmp, &s_base, &s_new);
+    p2_flush<NT, ScanT>(P2, G, D, smem, scap, s_spill != 0 || item.merge, scan_tmp, &s_base, &s_new);
     __syncthreads();
   }
   if (threadIdx.x == 0 && s_new) atomicAdd(G.counters, s_new);

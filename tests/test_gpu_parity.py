@@ -274,14 +274,67 @@ def test_partitioned_all_ones_key_heavy(scatter):
     assert gb.stats()["mode"] == 2
 
 
-def test_partitioned_skew_falls_back():
+def test_partitioned_skew_splits_heavy_partitions():
+    """Zipf(1.3) keys: a few keys hold a large share of the rows; their
+    partitions are cut into row ranges whose tables merge globally."""
     cb, agg = _cb()
     rng = np.random.default_rng(34)
     n = 2_000_000
     key = (rng.zipf(1.3, n) % 1_000_003).astype(np.int64)
     v = rng.integers(0, 1000, n).astype(np.int64)
-    run_both([cb.Column.from_numpy(key)], [(cb.Column.from_numpy(v), [agg.sum(), agg.count(), agg.max()])],
-             tuning={"force_mode": 2})
+    gb, *_ = run_both([cb.Column.from_numpy(key)], [(cb.Column.from_numpy(v), [agg.sum(), agg.count(), agg.max()])],
+                      tuning={"force_mode": 2})
+    assert gb.stats()["mode"] == 2
+
+
+@pytest.mark.parametrize("hot_frac", [0.5, 0.95])
+def test_partitioned_hot_key_warp_combined_updates(hot_frac):
+    """One key holds most rows: its partition is split and each warp combines
+    the hot key's values before one shared update, for every value type and
+    accumulator the partitioned path takes."""
+    cb, agg = _cb()
+    rng = np.random.default_rng(37)
+    n = 3_000_000
+    key = rng.integers(0, 400_000, n).astype(np.int64)
+    key[rng.random(n) < hot_frac] = 12345
+    cols = [
+        (rng.integers(-100, 100, n).astype(np.int8), None),
+        (rng.integers(-30000, 30000, n).astype(np.int16), rng.random(n) > 0.1),
+        (rng.integers(-2**31, 2**31 - 1, n).astype(np.int32), None),
+        (rng.integers(0, 2**63, n, dtype=np.uint64), rng.random(n) > 0.3),
+        (rng.normal(size=n).astype(np.float32), rng.random(n) > 0.1),
+        (rng.normal(size=n), None),
+        (rng.integers(0, 2, n).astype(np.uint8), None),
+    ]
+    types = [None, None, None, None, None, None, cb.TypeId.BOOL8]
+    aggs = [agg.sum(), agg.min(), agg.max(), agg.count(), agg.mean(), agg.sum_of_squares()]
+    reqs = []
+    for (v, m), t in zip(cols, types):
+        reqs.append((cb.Column.from_numpy(v, m, t) if t is not None else cb.Column.from_numpy(v, m), aggs))
+    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs[:4], tuning={"force_mode": 2})
+    assert gb.stats()["mode"] == 2
+    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs[4:], tuning={"force_mode": 2})
+    assert gb.stats()["mode"] == 2
+
+
+@pytest.mark.parametrize("include", [False, True])
+def test_zipf_pairs_two_word_keys(include):
+    """The shape of the high-cardinality benchmark at 4M rows: (int32, int64)
+    keys = divmod(p, 1000) with p Zipf-skewed, 5% nulls per key column."""
+    cb, agg = _cb()
+    rng = np.random.default_rng(36)
+    n = 4_000_000
+    u = rng.random(n)
+    a = 1.0 - 1.1
+    p = np.clip(np.floor((1.0 - u * (1.0 - 2_000_001.0 ** a)) ** (1.0 / a) - 1.0), 0, 1_999_999).astype(np.int64)
+    k1 = cb.Column.from_numpy((p // 1000).astype(np.int32), rng.random(n) >= 0.05)
+    k2 = cb.Column.from_numpy(p % 1000, rng.random(n) >= 0.05)
+    vi = rng.integers(0, 10**6, n, endpoint=True).astype(np.int64)
+    vf = rng.random(n)
+    aggs = [agg.sum(), agg.count(), agg.max()]
+    gb, *_ = run_both([k1, k2], [(cb.Column.from_numpy(vi), aggs), (cb.Column.from_numpy(vf), aggs)],
+                      include_null_keys=include)
+    assert gb.stats()["mode"] == 2
 
 
 def test_distributed_groupby_single_rank_with_engine():
