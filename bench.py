@@ -536,7 +536,7 @@ def run_serve(args):
                 "p99_s": float(np.percentile(lat, 99)), "completed": nq}
 
     def batched():
-        srv = cb.Server(memory_cap_bytes=150 << 30, workers=args.workers)
+        srv = cb.Server(memory_cap_bytes=150 << 30, workers=args.workers, direct_rows=args.direct_rows)
         ids = [None] * nq
         done = threading.Event()
 
@@ -550,16 +550,17 @@ def run_serve(args):
 
         th = threading.Thread(target=collector)
         th.start()
-        t0 = time.perf_counter()
-        for i in range(nq):
-            now = time.perf_counter() - t0
-            if now < arrivals[i]:
-                time.sleep(arrivals[i] - now)
-            ids[i] = srv.submit(*qs[i])
-        th.join()
-        st = srv.stats()
-        srv.close()
-        return st
+        try:
+            t0 = time.perf_counter()
+            for i in range(nq):
+                now = time.perf_counter() - t0
+                if now < arrivals[i]:
+                    time.sleep(arrivals[i] - now)
+                ids[i] = srv.submit(*qs[i])
+            th.join()
+            return srv.stats()
+        finally:
+            srv.close()
 
     b = batched()
     p = plain()
@@ -722,7 +723,9 @@ def main():
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--duration", type=float, default=5.0)
     ap.add_argument("--pool", type=int, default=16)
-    ap.add_argument("--workers", type=int, default=2)
+    ap.add_argument("--workers", type=int, default=4)
+    ap.add_argument("--direct-rows", type=int, default=0,
+                    help="serve: queries with at least this many rows run alone (0: server default)")
     args = ap.parse_args()
     if args.workload == "batch" and args.impl == "engine":
         return run_batch(args)

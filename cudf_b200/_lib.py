@@ -63,7 +63,8 @@ class GbBatchStats(ctypes.Structure):
 
 class GbServerOptions(ctypes.Structure):
     _fields_ = [("memory_cap_bytes", ctypes.c_int64), ("max_batch_queries", ctypes.c_int32),
-                ("max_batch_rows", ctypes.c_int64), ("workers", ctypes.c_int32)]
+                ("max_batch_rows", ctypes.c_int64), ("workers", ctypes.c_int32),
+                ("direct_rows", ctypes.c_int64), ("direct_groups", ctypes.c_int64)]
 
 
 class GbQueryInfo(ctypes.Structure):

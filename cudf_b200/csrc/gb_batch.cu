@@ -502,7 +502,7 @@ std::vector<int64_t> batch_estimate_groups(const std::vector<std::vector<Column>
   d_stats.get(A, (size_t)ninst * 16, stream);
   ck(cudaMemcpyAsync(d_insts.p, insts.data(), sizeof(BatchInst) * ninst, cudaMemcpyHostToDevice, stream), "h2d");
   size_t sm = (size_t)kSampleSlots * 32;
-  ck(cudaFuncSetAttribute(k_batch_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), "attr");
+  allow_max_smem((const void*)k_batch_sample);
   k_batch_sample<<<ninst, 256, sm, stream>>>(P, (const BatchInst*)d_insts.p, (unsigned int*)d_stats.p);
   ck(cudaGetLastError(), "sketch launch");
   std::vector<unsigned int> st((size_t)ninst * 4);
@@ -600,7 +600,7 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
   if (bo.est_groups.empty()) {
     B.d_stats.get(A, (size_t)ninst * 16, stream);
     size_t sm = (size_t)kSampleSlots * 32;
-    ck(cudaFuncSetAttribute(k_batch_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), "attr");
+    allow_max_smem((const void*)k_batch_sample);
     k_batch_sample<<<ninst, 256, sm, stream>>>(B.P, (const BatchInst*)B.d_insts.p, (unsigned int*)B.d_stats.p);
     ck(cudaGetLastError(), "batch sample");
     ck(cudaMemcpyAsync(st.data(), B.d_stats.p, st.size() * 4, cudaMemcpyDeviceToHost, stream), "d2h");
@@ -664,7 +664,7 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
   if (!B.h_counters) ck(cudaMallocHost((void**)&B.h_counters, (size_t)ninst * B.counter_words * 4), "cudaMallocHost");
   // launch shapes
   B.smem_bytes = scap_max * stride;
-  ck(cudaFuncSetAttribute(k_batch_aggregate, cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem_bytes), "attr");
+  allow_max_smem((const void*)k_batch_aggregate);
   int bps = 0;
   ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_aggregate, kBatchThreads, B.smem_bytes), "occ");
   B.grid_agg = (int)std::min<int64_t>(std::max<int64_t>(1, (int64_t)B.tiles.size()), 1 << 30);

@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -429,6 +430,23 @@ static void build_template(const Plan& P, SlotTemplate& t)
   }
 }
 
+void allow_max_smem(const void* kernel)
+{
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  ck(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({dev, kernel})) return;
+  int optin = 0;
+  ck(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "smem attr");
+  cudaFuncAttributes fa;
+  ck(cudaFuncGetAttributes(&fa, kernel), "func attr");
+  ck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes),
+     "smem attr");
+  done.insert({dev, kernel});
+}
+
 // ---------------------------------------------------------------------------
 namespace {
 thread_local uint32_t* t_pinned = nullptr;
@@ -439,9 +457,12 @@ cudaEvent_t* events()
     for (auto& e : t_ev) ck(cudaEventCreate(&e), "cudaEventCreate");
   return t_ev;
 }
+// Per-thread pinned host words: [0, 1024) counters read back by the host,
+// [1024, 1024 + 2^kHllBits + 2^kBucketBits) the key sketch.
+constexpr size_t kPinnedWords = 1024 + (size_t(1) << kHllBits) + (size_t(1) << kBucketBits);
 uint32_t* pinned()
 {
-  if (!t_pinned) ck(cudaMallocHost((void**)&t_pinned, 4096), "cudaMallocHost");
+  if (!t_pinned) ck(cudaMallocHost((void**)&t_pinned, kPinnedWords * 4), "cudaMallocHost");
   return t_pinned;
 }
 
@@ -553,7 +574,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
        "memset sketch");
     {
       const size_t sm = sketch_smem();
-      ck(cudaFuncSetAttribute(k_sketch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), "attr");
+      allow_max_smem((const void*)k_sketch);
       int grid = grid_for((const void*)k_sketch, 512, sm, 0);
       grid = (int)std::min<int64_t>(grid, (n + 511) / 512);
       k_sketch<<<grid, 512, sm, stream>>>(P, hll, bk);
@@ -561,11 +582,12 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     st.kernels += 1;
     ck(cudaGetLastError(), "sketch launch");
     mark("sketch launched");
-    std::vector<uint32_t> regs((size_t)1 << kHllBits);
-    buckets.resize((size_t)1 << kBucketBits);
-    ck(cudaMemcpyAsync(regs.data(), hll, regs.size() * 4, cudaMemcpyDeviceToHost, stream), "sketch d2h");
-    ck(cudaMemcpyAsync(buckets.data(), bk, buckets.size() * 4, cudaMemcpyDeviceToHost, stream), "sketch d2h");
+    uint32_t* hs = host + 1024;  // registers then buckets, adjacent on the device too
+    ck(cudaMemcpyAsync(hs, hll, ((size_t(1) << kHllBits) + (size_t(1) << kBucketBits)) * 4, cudaMemcpyDeviceToHost,
+                       stream), "sketch d2h");
     ck(cudaStreamSynchronize(stream), "sketch sync");
+    std::vector<uint32_t> regs(hs, hs + (size_t(1) << kHllBits));
+    buckets.assign(hs + (size_t(1) << kHllBits), hs + (size_t(1) << kHllBits) + (size_t(1) << kBucketBits));
     S.put(hll);
     exact_buckets = true;
     int64_t valid_rows = 0;
@@ -697,7 +719,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     {
       auto launch = [&](auto kern, int nt, int rpt) {
         size_t psmem = part_scatter_smem(P.key_words, nt * rpt, nparts);
-        ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem), "attr");
+        allow_max_smem((const void*)kern);
         int grid = grid_for((const void*)kern, nt, psmem, 0);
         kern<<<grid, nt, psmem, stream>>>(P, A);
       };
@@ -781,7 +803,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
         Ai.items = d_items + first;
         Ai.nitems = count;
         Ai.work = work;
-        ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2), "attr");
+        allow_max_smem((const void*)kern);
         int grid = grid_for((const void*)kern, nt, sm2, 0);
         grid = std::min(grid, count);
         kern<<<grid, nt, sm2, stream>>>(P2, Ai, G, D, scap2, sfill2, tmpl);
@@ -865,7 +887,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       if (opt.profile) ck(cudaEventRecord(events()[0], stream), "event");
       if (mode == 1) {
         size_t sm = (size_t)scap * P.slot_bytes;
-        ck(cudaFuncSetAttribute(k_aggregate<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), "smem attr");
+        allow_max_smem((const void*)k_aggregate<true>);
         int grid = grid_for((const void*)k_aggregate<true>, block, sm, opt.blocks_per_sm);
         grid = (int)std::min<int64_t>(grid, (n + block - 1) / block);
         k_aggregate<true><<<grid, block, sm, stream>>>(P, G, scap, sfill, tmpl);

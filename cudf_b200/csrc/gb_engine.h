@@ -116,4 +116,11 @@ int type_width(int type_id);
 bool valid_agg(int type_id, int kind);
 int target_type(int type_id, int kind);
 
+// Lets `kernel` take up to the device's opt-in shared memory per block.  Set
+// once per (device, kernel) at that maximum, not per launch at the size the
+// launch needs: engine calls on several host threads launch the same kernels
+// with different shared-memory sizes, and a per-launch attribute set by one
+// thread could be lowered by another between its set and its launch.
+void allow_max_smem(const void* kernel);
+
 }  // namespace gb

@@ -50,7 +50,8 @@ struct Query {
   std::string error;
   std::shared_ptr<Batch> batch;  // keeps the result buffers alive
   int index_in_batch = 0;
-  std::shared_ptr<Result> direct;  // queries run alone (large, many groups)
+  bool run_direct = false;          // routed to the single-query engine
+  std::shared_ptr<Result> direct;   // its result
   ~Query()
   {
     if (direct) direct->release();
@@ -82,8 +83,6 @@ struct Server {
   double first_arrive = -1, last_done = 0;
   double sketch_s = 0, prepare_s = 0, run_s = 0, trial_s = 0;
   int64_t trial_rounds = 0, direct_runs = 0;
-  int64_t opt_direct_rows = 4 << 20;     // queries at least this long ...
-  int64_t opt_direct_groups = 4096;      // ... with more groups than this run alone
   cudaStream_t sketch_stream = nullptr;
 
   // device-side sketch of a set of queries: estimated groups per query, one
@@ -184,12 +183,28 @@ struct Server {
           if (rows >= opt.max_batch_rows) break;
         }
         if (!admitted.empty()) {
-          // do not queue more than one batch ahead of the workers
-          cv_worker.wait(lk, [&] { return stop || (int64_t)work.size() < std::max(1, idle_workers); });
-          WorkItem w;
-          w.queries = std::move(admitted);
-          work.push_back(std::move(w));
-          cv_worker.notify_all();
+          // large or many-group queries run alone through the single-query
+          // engine (hash-partitioned for many groups), one work item each so
+          // idle workers take them in parallel; the rest share one batched
+          // launch.  Never queue more than one item per idle worker ahead.
+          std::vector<WorkItem> items;
+          WorkItem batched;
+          for (auto& q : admitted) {
+            q->run_direct = q->keys[0].size >= opt.direct_rows || q->est_groups > opt.direct_groups;
+            if (q->run_direct) {
+              WorkItem w;
+              w.queries.push_back(q);
+              items.push_back(std::move(w));
+            } else {
+              batched.queries.push_back(q);
+            }
+          }
+          if (!batched.queries.empty()) items.push_back(std::move(batched));
+          for (auto& w : items) {
+            cv_worker.wait(lk, [&] { return stop || (int64_t)work.size() < std::max(1, idle_workers); });
+            work.push_back(std::move(w));
+            cv_worker.notify_all();
+          }
         }
       }
     }
@@ -233,12 +248,13 @@ struct Server {
       for (auto& kv : groups) {
         std::vector<std::shared_ptr<Query>> rest;
         for (auto& q : kv.second) {
-          if (q->keys[0].size >= opt_direct_rows && q->est_groups > opt_direct_groups) {
+          if (q->run_direct) {
             std::string err;
             auto R = std::make_shared<Result>();
             try {
+              // the engine's own full-pass sketch sizes the tables (the
+              // dispatcher's sample only routes the query)
               Options o;
-              o.groups_hint = q->est_groups * 2;
               *R = aggregate(q->keys, q->null_policy, q->reqs, s, default_allocator(), o, nullptr);
             } catch (const std::exception& ex) {
               err = ex.what();
@@ -368,12 +384,16 @@ int gb_server_create(const gb_server_options* opt, gb_server** out)
     S.opt.memory_cap_bytes = 150ll << 30;
     S.opt.max_batch_queries = 256;
     S.opt.max_batch_rows = 400ll << 20;
-    S.opt.workers = 2;
+    S.opt.workers = 4;
+    S.opt.direct_rows = 64 << 10;
+    S.opt.direct_groups = 64 << 10;
     if (opt) {
       if (opt->memory_cap_bytes > 0) S.opt.memory_cap_bytes = opt->memory_cap_bytes;
       if (opt->max_batch_queries > 0) S.opt.max_batch_queries = opt->max_batch_queries;
       if (opt->max_batch_rows > 0) S.opt.max_batch_rows = opt->max_batch_rows;
       if (opt->workers > 0) S.opt.workers = std::min(8, opt->workers);
+      if (opt->direct_rows > 0) S.opt.direct_rows = opt->direct_rows;
+      if (opt->direct_groups > 0) S.opt.direct_groups = opt->direct_groups;
     }
     if (cudaGetDevice(&S.device) != cudaSuccess) throw gb::Error(gb::ERR_CUDA, "cudaGetDevice failed");
     S.threads.emplace_back([&S] { S.dispatcher(); });

@@ -9,8 +9,10 @@ columns (the C++ loop in csrc/gb_server.cu).
 """
 from __future__ import annotations
 
+import atexit
 import ctypes
 import threading
+import weakref
 from typing import List
 
 from . import _lib
@@ -19,14 +21,31 @@ from .groupby import GroupByRequest
 from .types import NullPolicy
 
 
+# Servers still open at interpreter exit are closed first: their C++ worker
+# threads must be joined before the process tears down the CUDA runtime.
+_OPEN: "weakref.WeakSet[Server]" = weakref.WeakSet()
+
+
+@atexit.register
+def _close_open_servers():
+    for s in list(_OPEN):
+        try:
+            s.close()
+        except Exception:
+            pass
+
+
 class Server:
     def __init__(self, memory_cap_bytes: int = 150 << 30, max_batch_queries: int = 256,
-                 max_batch_rows: int = 400 << 20, workers: int = 2):
+                 max_batch_rows: int = 400 << 20, workers: int = 4, direct_rows: int = 0,
+                 direct_groups: int = 0):
         L = _lib.lib()
-        o = _lib.GbServerOptions(memory_cap_bytes, max_batch_queries, max_batch_rows, workers)
+        o = _lib.GbServerOptions(memory_cap_bytes, max_batch_queries, max_batch_rows, workers,
+                                 direct_rows, direct_groups)
         h = ctypes.c_void_p()
         _lib.check(L.gb_server_create(ctypes.byref(o), ctypes.byref(h)))
         self._h = h
+        _OPEN.add(self)
         self._mu = threading.Lock()
         self._live = {}  # query id -> (columns kept alive, aggregation counts)
 

@@ -231,7 +231,10 @@ typedef struct gb_server_options {
   int64_t memory_cap_bytes;   /* admission cap (default 150 GiB) */
   int32_t max_batch_queries;  /* queries per batched launch (default 256) */
   int64_t max_batch_rows;     /* rows per batched launch (default 400 Mi) */
-  int32_t workers;            /* worker threads / streams (default 2) */
+  int32_t workers;            /* worker threads / streams (default 4) */
+  int64_t direct_rows;        /* queries with at least this many rows run alone through the
+                                 single-query engine (default 64 Ki) ... */
+  int64_t direct_groups;      /* ... as do queries with more estimated groups (default 64 Ki) */
 } gb_server_options;
 typedef struct gb_query_info {
   int32_t status;             /* 2 done, 3 failed */

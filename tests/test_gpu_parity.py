@@ -365,3 +365,48 @@ def test_distributed_groupby_single_rank_with_engine():
     gk = [(mk[0][0].cpu().numpy(), None)]
     gr = [[(d.cpu().numpy(), None if vv is None else vv.cpu().numpy()) for d, vv in per] for per in mres]
     compare(o, gk, gr, [[int(x) for x in kinds]] * 2, None)
+
+
+def test_concurrent_calls_on_separate_streams():
+    """Four host threads, each with its own stream, run groupbys of different
+    modes (and so different shared-memory sizes for the same kernels) at the
+    same time; every result equals the same call made alone."""
+    import threading
+    cb, agg = _cb()
+    rng = np.random.default_rng(38)
+    shapes = [(1_500_000, 300_000), (200_000, 50), (2_500_000, 1_000_000), (800_000, 5_000)]
+    inputs = []
+    for n, card in shapes:
+        k = rng.integers(0, card, n).astype(np.int64) * 7919
+        v = rng.integers(-10**9, 10**9, n).astype(np.int64)
+        inputs.append((cb.Column.from_numpy(k), cb.Column.from_numpy(v, rng.random(n) > 0.1)))
+    aggs = [agg.sum(), agg.count(), agg.min(), agg.max()]
+
+    def run(i, out):
+        k, v = inputs[i]
+        s = torch.cuda.Stream()
+        with torch.cuda.stream(s):
+            for _ in range(3):
+                uk, res = cb.GroupBy(cb.Table([k])).aggregate([cb.GroupByRequest(v, aggs)], stream=s)
+            s.synchronize()
+        out[i] = (uk, res)
+
+    alone = [None] * 4
+    for i in range(4):
+        run(i, alone)
+    mixed = [None] * 4
+    th = [threading.Thread(target=run, args=(i, mixed)) for i in range(4)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for i in range(4):
+        (ka, ra), (km, rm) = alone[i], mixed[i]
+        a_keys, a_vals = ka[0].to_numpy()[0], [c.to_numpy() for c in ra[0].columns]
+        m_keys, m_vals = km[0].to_numpy()[0], [c.to_numpy() for c in rm[0].columns]
+        oa, om = np.argsort(a_keys), np.argsort(m_keys)
+        assert np.array_equal(a_keys[oa], m_keys[om])
+        for (av, avv), (mv, mvv) in zip(a_vals, m_vals):
+            assert np.array_equal(av[oa], mv[om])
+            if avv is not None:
+                assert np.array_equal(avv[oa], mvv[om])
