@@ -731,7 +731,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
         case 4: kw1 ? launch(k_part_scatter<1, 8, 512, 3>, 512, 8) : launch(k_part_scatter<2, 8, 512, 3>, 512, 8); break;
         case 5: kw1 ? launch(k_part_scatter<1, 4, 1024, 2, false>, 1024, 4) : launch(k_part_scatter<2, 4, 1024, 2, false>, 1024, 4); break;
         case 6: kw1 ? launch(k_part_scatter<1, 8, 256, 4>, 256, 8) : launch(k_part_scatter<2, 8, 256, 4>, 256, 8); break;
-        default: kw1 ? launch(k_part_scatter<1, 8, 512, 3, false>, 512, 8) : launch(k_part_scatter<2, 8, 512, 3, false>, 512, 8); break;
+        default: kw1 ? launch(k_part_scatter<1, 8, 512, 3, false>, 512, 8) : launch(k_part_scatter<2, 8, 512, 2, false>, 512, 8); break;
       }
     }
     ++st.kernels;

@@ -71,7 +71,7 @@ __device__ __forceinline__ void prefetch_l2(const void* p)
 //      the stage at their sorted position and written out in sorted order
 //      (consecutive threads, consecutive rows of a run).  The next column's
 //      loads are issued before the current column's write-out.
-// Shared memory: stage[tile * 8*KW] | psort u16[tile] | hist u32[nparts] |
+// Shared memory: stage[tile * 8] | psort u16[tile] | hist u32[nparts] |
 //                send u32[nparts] | delta i64[nparts]
 template <int KW, int RPT, int NT, int MINB, bool PF = true>
 __global__ void __launch_bounds__(NT, MINB) k_part_scatter(const __grid_constant__ Plan P,
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(NT, MINB) k_part_scatter(const __grid_constant
   static_assert(TILE <= 65536, "sorted positions are 16-bit");
   extern __shared__ __align__(16) uint8_t sh[];
   uint8_t* stage = sh;
-  uint16_t* psort = (uint16_t*)(sh + (size_t)TILE * 8 * KW);
+  uint16_t* psort = (uint16_t*)(sh + (size_t)TILE * 8);
   unsigned int* hist = (unsigned int*)(psort + TILE);
   unsigned int* send = hist + A.nparts;
   long long* delta = (long long*)(send + A.nparts + (A.nparts & 1));
@@ -178,6 +178,9 @@ __global__ void __launch_bounds__(NT, MINB) k_part_scatter(const __grid_constant
       pr[k] = (p << 16) | s;
       psort[s] = (uint16_t)p;
     }
+    // two-word keys go through the 8-byte stage one word at a time (word 1
+    // waits in registers), which halves the stage and lets two CTAs share an SM
+    uint64_t kw1[KW == 2 ? RPT : 1];
     if (plain_key) {
       uint64_t k0[RPT];
 #pragma unroll
@@ -191,8 +194,8 @@ __global__ void __launch_bounds__(NT, MINB) k_part_scatter(const __grid_constant
         if (pr[k] == 0xFFFFFFFFu) continue;
         uint64_t w0 = 0, w1 = 0;
         pack_key(P, t0 + k * NT + threadIdx.x, w0, w1);
-        if (KW == 1) ((uint64_t*)stage)[pr[k] & 0xFFFFu] = w0;
-        else ((ulonglong2*)stage)[pr[k] & 0xFFFFu] = make_ulonglong2(w0, w1);
+        ((uint64_t*)stage)[pr[k] & 0xFFFFu] = w0;
+        if (KW == 2) kw1[k] = w1;
       }
     }
     // first value column's loads in flight with the key write-out
@@ -211,8 +214,19 @@ __global__ void __launch_bounds__(NT, MINB) k_part_scatter(const __grid_constant
       const unsigned p = psort[s];
       if ((unsigned)s >= send[p]) continue;
       const int64_t g = delta[p] + s;
-      if (KW == 1) A.keys[g] = ((const uint64_t*)stage)[s];
-      else ((ulonglong2*)A.keys)[g] = ((const ulonglong2*)stage)[s];
+      A.keys[KW * g] = ((const uint64_t*)stage)[s];
+    }
+    if (KW == 2) {
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < RPT; ++k)
+        if (pr[k] != 0xFFFFFFFFu) ((uint64_t*)stage)[pr[k] & 0xFFFFu] = kw1[k];
+      __syncthreads();
+      for (int s = threadIdx.x; s < nvalid; s += NT) {
+        const unsigned p = psort[s];
+        if ((unsigned)s >= send[p]) continue;
+        A.keys[2 * (delta[p] + s) + 1] = ((const uint64_t*)stage)[s];
+      }
     }
     // validity bytes of this thread's rows, four to a register
     uint32_t vb[(RPT + 3) / 4];
@@ -280,7 +294,8 @@ __global__ void __launch_bounds__(NT, MINB) k_part_scatter(const __grid_constant
 // shared-memory bytes of k_part_scatter for a tile of `tile` rows
 inline size_t part_scatter_smem(int kw, int tile, int nparts)
 {
-  return (size_t)tile * 8 * kw + (size_t)tile * 2 + (size_t)nparts * 8 + 8 + (size_t)nparts * 8;
+  (void)kw;
+  return (size_t)tile * 8 + (size_t)tile * 2 + (size_t)nparts * 8 + 8 + (size_t)nparts * 8;
 }
 
 // Shared-memory find-or-insert (bounded probes); null when the key does not
