@@ -10,6 +10,20 @@ from .serving import Server
 from .types import Kind, NullPolicy, Sorted, TypeId
 from .frame import DataFrame
 
+def _install_tuning():
+    """Installs the measured per-size-bucket tuning rules shipped with the
+    package, when present (see cudf_b200.autotune)."""
+    import os
+    from . import autotune
+    if os.path.exists(autotune.TUNING_FILE):
+        try:
+            autotune.load(autotune.TUNING_FILE)
+        except Exception:  # the engine library reports itself when it is used
+            pass
+
+
+_install_tuning()
+
 __all__ = ["aggregation", "BatchGroupBy", "Column", "DataFrame", "HostStaging", "Table", "GroupBy", "GroupByRequest",
            "Kind", "NullPolicy", "Server", "Sorted", "TypeId"]
 __version__ = "0.1.0"

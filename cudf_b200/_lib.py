@@ -52,7 +52,11 @@ class GbStats(ctypes.Structure):
     _fields_ = [("est_groups", ctypes.c_int64), ("capacity", ctypes.c_int64), ("mode", ctypes.c_int32),
                 ("retries", ctypes.c_int32), ("kernels", ctypes.c_int32),
                 ("agg_kernel_ms", ctypes.c_double), ("compact_ms", ctypes.c_double),
-                ("scatter_ms", ctypes.c_double)]
+                ("scatter_ms", ctypes.c_double), ("rule", ctypes.c_int32)]
+
+
+class GbTuningRule(ctypes.Structure):
+    _fields_ = [("max_rows", ctypes.c_int64), ("max_groups", ctypes.c_int64), ("tuning", GbTuning)]
 
 
 class GbBatchStats(ctypes.Structure):
@@ -112,6 +116,7 @@ SIGNATURES = {
     "gb_is_valid_aggregation": (ctypes.c_int32, [ctypes.c_int32, ctypes.c_int32]),
     "gb_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GbTuning)]),
     "gb_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GbStats)]),
+    "gb_set_tuning_rules": (ctypes.c_int, [ctypes.POINTER(GbTuningRule), ctypes.c_int32]),
     "gb_version": (ctypes.c_char_p, []),
     "gb_batch_prepare": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(GbColumn), ctypes.c_int32, ctypes.c_int32,
                                         ctypes.POINTER(GbRequest), ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,

@@ -1,0 +1,183 @@
+"""Per-size-bucket autotuner for the engine's launch parameters.
+
+The engine's kernels have tunables (mode thresholds, shared-memory table size
+and fill, global-table load factor, the partition pass's launch shape).  The
+best values depend on the call's size: rows and distinct groups.  This module
+times candidate settings on synthetic inputs of each (rows, groups) bucket
+with CUDA events, keeps the fastest, and installs the result as process-wide
+rules (``gb_set_tuning_rules``): a call takes the first rule whose bucket
+covers its row count and its estimated group count, after the engine's own
+sketch has estimated the groups.
+
+    python -m cudf_b200.autotune --out cudf_b200/tuning_b200.json   # on a B200
+
+``cudf_b200`` installs ``tuning_b200.json`` (next to this file) at import
+when it exists; ``load(path)`` / ``clear()`` change that at run time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import time
+from typing import Dict, List, Optional, Sequence, Tuple
+
+from . import _lib
+
+TUNING_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning_b200.json")
+
+# fields of a rule's tuning, with the value meaning "unset" in gb_tuning
+_UNSET = {"block": -1, "blocks_per_sm": -1, "smem_bytes": -1, "smem_fill_pct": -1, "smem_max_groups": -1,
+          "load_factor_pct": -1, "force_mode": -2, "groups_hint": -1, "profile": -1, "scatter": -1}
+
+# default buckets: row counts x group counts seen by the benchmark shapes
+DEFAULT_BUCKETS = [
+    (1 << 20, 1 << 10), (1 << 20, 1 << 17), (1 << 20, 1 << 20),
+    (1 << 24, 1 << 10), (1 << 24, 1 << 17), (1 << 24, 1 << 22),
+    (1 << 27, 1 << 10), (1 << 27, 1 << 17), (1 << 27, 1 << 20), (1 << 27, 1 << 24),
+]
+
+# candidate settings per stage of the search (coordinate descent)
+_MODES = [{"force_mode": -1}, {"force_mode": 0}, {"force_mode": 1}, {"force_mode": 2}]
+_SCATTER = [{"scatter": s} for s in range(7)]
+_SMEM = [{"smem_bytes": b, "smem_fill_pct": f} for b in (48 << 10, 96 << 10, 160 << 10) for f in (50, 70)]
+_LOAD = [{"load_factor_pct": p} for p in (40, 50, 70)]
+
+
+def _tuning_struct(t: Dict[str, int]) -> _lib.GbTuning:
+    vals = dict(_UNSET)
+    vals.update(t)
+    return _lib.GbTuning(*[int(vals[name]) for name, _ in _lib.GbTuning._fields_])
+
+
+def set_rules(rules: Sequence[Dict]) -> None:
+    """Installs rules [{"max_rows", "max_groups", "tuning": {field: value}}]
+    in order (the first match applies)."""
+    arr = (_lib.GbTuningRule * max(1, len(rules)))()
+    for i, r in enumerate(rules):
+        arr[i] = _lib.GbTuningRule(int(r["max_rows"]), int(r["max_groups"]), _tuning_struct(r.get("tuning", {})))
+    _lib.check(_lib.lib().gb_set_tuning_rules(arr, len(rules)))
+
+
+def clear() -> None:
+    _lib.check(_lib.lib().gb_set_tuning_rules(None, 0))
+
+
+def save(rules: Sequence[Dict], path: str, meta: Optional[Dict] = None) -> None:
+    with open(path, "w") as f:
+        json.dump({"rules": list(rules), "meta": meta or {}}, f, indent=1)
+
+
+def load(path: str = TUNING_FILE) -> List[Dict]:
+    with open(path) as f:
+        rules = json.load(f)["rules"]
+    set_rules(rules)
+    return rules
+
+
+def order_rules(rules: Sequence[Dict]) -> List[Dict]:
+    """Smallest buckets first, so the first match is the tightest bucket."""
+    return sorted(rules, key=lambda r: (int(r["max_rows"]), int(r["max_groups"])))
+
+
+# -- the search (needs a GPU) ---------------------------------------------------
+def _workload(rows: int, groups: int, seed: int = 0):
+    """Synthetic bucket input: int64 keys uniform over `groups` distinct
+    values; int64, float64 and float32 values, 10% nulls each; sum, count,
+    min, max, mean per value column (the 100M-row benchmark's request)."""
+    import torch
+    from . import aggregation as agg
+    from .column import Column, Table, pack_mask
+    from .groupby import GroupByRequest
+    from .types import TypeId
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    distinct = torch.randint(-2**62, 2**62, (groups,), device="cuda", generator=g, dtype=torch.int64)
+    key = distinct[torch.randint(0, groups, (rows,), device="cuda", generator=g)]
+    vals = [torch.randint(-10**9, 10**9, (rows,), device="cuda", generator=g, dtype=torch.int64),
+            torch.randn(rows, device="cuda", generator=g, dtype=torch.float64),
+            torch.rand(rows, device="cuda", generator=g, dtype=torch.float32)]
+    masks = [pack_mask(torch.rand(rows, device="cuda", generator=g) >= 0.1) for _ in range(3)]
+    aggs = [agg.sum(), agg.count(), agg.min(), agg.max(), agg.mean()]
+    reqs = [GroupByRequest(Column(t, v, m), aggs)
+            for t, v, m in zip((TypeId.INT64, TypeId.FLOAT64, TypeId.FLOAT32), vals, masks)]
+    return Table([Column(TypeId.INT64, key)]), reqs
+
+
+def _time(keys, reqs, tuning: Dict[str, int], steps: int) -> float:
+    import torch
+    from .groupby import GroupBy
+    gb = GroupBy(keys)
+    if tuning:
+        gb.set_tuning(**tuning)
+    gb.aggregate(reqs)  # warm (allocator pool, first launches)
+    stream = torch.cuda.current_stream()
+    times = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        gb.aggregate(reqs)
+        b.record(stream)
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    times.sort()
+    return times[len(times) // 2]
+
+
+def tune_bucket(rows: int, groups: int, steps: int = 5, verbose: bool = False) -> Tuple[Dict[str, int], Dict]:
+    """Coordinate descent: mode, then (for the chosen mode) the partition
+    launch shape or the shared-memory table, then the load factor."""
+    keys, reqs = _workload(rows, groups)
+    log = {}
+    best: Dict[str, int] = {}
+    best_ms = _time(keys, reqs, best, steps)
+    log["default"] = best_ms
+    for stage in (_MODES, _SCATTER, _SMEM, _LOAD):
+        if stage is _SCATTER and best.get("force_mode", -1) not in (-1, 2):
+            continue
+        if stage is _SMEM and best.get("force_mode", -1) not in (-1, 1):
+            continue
+        for cand in stage:
+            t = dict(best)
+            t.update(cand)
+            try:
+                ms = _time(keys, reqs, t, steps)
+            except Exception as e:  # a setting the call rejects is skipped
+                log[json.dumps(t)] = str(e)
+                continue
+            log[json.dumps(t)] = ms
+            if ms < best_ms * 0.98:
+                best, best_ms = t, ms
+    if verbose:
+        print(f"rows={rows} groups={groups}: {best} {best_ms:.3f} ms", flush=True)
+    return best, {"best_ms": best_ms, "trials": log}
+
+
+def tune(buckets: Sequence[Tuple[int, int]] = DEFAULT_BUCKETS, steps: int = 5, verbose: bool = False):
+    clear()
+    rules, meta = [], {"when": time.strftime("%Y-%m-%dT%H:%M:%S"), "buckets": {}}
+    for rows, groups in buckets:
+        t, info = tune_bucket(rows, groups, steps, verbose)
+        rules.append({"max_rows": rows, "max_groups": groups, "tuning": t})
+        meta["buckets"][f"{rows}x{groups}"] = info
+    return order_rules(rules), meta
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--out", default=TUNING_FILE)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--max-rows", type=int, default=1 << 27, help="skip buckets with more rows")
+    args = ap.parse_args()
+    import torch
+    name = torch.cuda.get_device_name(0)
+    buckets = [b for b in DEFAULT_BUCKETS if b[0] <= args.max_rows]
+    rules, meta = tune(buckets, args.steps, verbose=True)
+    meta["device"] = name
+    save(rules, args.out, meta)
+    print(f"wrote {len(rules)} rules to {args.out}")
+
+
+if __name__ == "__main__":
+    main()

@@ -152,27 +152,56 @@ void gb_result_free(gb_result* res)
 
 const char* gb_last_error(void) { return t_err.c_str(); }
 
+// Copies the fields of `t` that are set into `o`; returns their OPT_* bits.
+static uint32_t apply_tuning(const gb_tuning* t, gb::Options& o)
+{
+  uint32_t m = 0;
+  if (t->block > 0) {
+    if (t->block % 32 || t->block > 1024) throw gb::Error(gb::ERR_LOGIC, "block must be a multiple of 32, <= 1024");
+    o.block = t->block;
+    m |= gb::OPT_BLOCK;
+  }
+  if (t->blocks_per_sm >= 0) o.blocks_per_sm = t->blocks_per_sm, m |= gb::OPT_BPS;
+  if (t->smem_bytes >= 0) o.smem_bytes = t->smem_bytes, m |= gb::OPT_SMEM;
+  if (t->smem_fill_pct > 0) o.smem_fill = std::min(95, t->smem_fill_pct) / 100.0, m |= gb::OPT_FILL;
+  if (t->smem_max_groups >= 0) o.smem_max_groups = t->smem_max_groups, m |= gb::OPT_SMEM_MAX;
+  if (t->load_factor_pct > 0) o.load_factor = std::min(90, t->load_factor_pct) / 100.0, m |= gb::OPT_LOAD;
+  if (t->force_mode >= -1) {
+    if (t->force_mode > 2) throw gb::Error(gb::ERR_LOGIC, "force_mode must be in [-1, 2]");
+    o.force_mode = t->force_mode;
+    m |= gb::OPT_MODE;
+  }
+  if (t->groups_hint >= 0) o.groups_hint = t->groups_hint;
+  if (t->profile >= 0) o.profile = t->profile;
+  if (t->scatter >= 0) {
+    if (t->scatter > 6) throw gb::Error(gb::ERR_LOGIC, "scatter must be in [0, 6]");
+    o.scatter = t->scatter;
+    m |= gb::OPT_SCATTER;
+  }
+  return m;
+}
+
 int gb_set_tuning(gb_handle* h, const gb_tuning* t)
 {
   return guarded([&] {
     if (!h || !t) throw gb::Error(gb::ERR_LOGIC, "null handle or tuning");
-    gb::Options& o = h->opt;
-    if (t->block > 0) {
-      if (t->block % 32 || t->block > 1024) throw gb::Error(gb::ERR_LOGIC, "block must be a multiple of 32, <= 1024");
-      o.block = t->block;
+    h->opt.set_mask |= apply_tuning(t, h->opt);
+  });
+}
+
+int gb_set_tuning_rules(const gb_tuning_rule* rules, int32_t num_rules)
+{
+  return guarded([&] {
+    if (num_rules < 0 || (num_rules > 0 && !rules)) throw gb::Error(gb::ERR_LOGIC, "bad tuning rules");
+    std::vector<gb::TuningRule> v;
+    for (int i = 0; i < num_rules; ++i) {
+      gb::TuningRule r;
+      r.max_rows = rules[i].max_rows;
+      r.max_groups = rules[i].max_groups;
+      r.mask = apply_tuning(&rules[i].tuning, r.opt);
+      v.push_back(r);
     }
-    if (t->blocks_per_sm >= 0) o.blocks_per_sm = t->blocks_per_sm;
-    if (t->smem_bytes >= 0) o.smem_bytes = t->smem_bytes;
-    if (t->smem_fill_pct > 0) o.smem_fill = std::min(95, t->smem_fill_pct) / 100.0;
-    if (t->smem_max_groups >= 0) o.smem_max_groups = t->smem_max_groups;
-    if (t->load_factor_pct > 0) o.load_factor = std::min(90, t->load_factor_pct) / 100.0;
-    if (t->force_mode >= -1) o.force_mode = t->force_mode;
-    if (t->groups_hint >= 0) o.groups_hint = t->groups_hint;
-    if (t->profile >= 0) o.profile = t->profile;
-    if (t->scatter >= 0) {
-      if (t->scatter > 6) throw gb::Error(gb::ERR_LOGIC, "scatter must be in [0, 6]");
-      o.scatter = t->scatter;
-    }
+    gb::set_tuning_rules(v);
   });
 }
 
@@ -188,6 +217,7 @@ int gb_get_stats(const gb_handle* h, gb_stats* out)
     out->agg_kernel_ms = h->stats.agg_kernel_ms;
     out->compact_ms = h->stats.compact_ms;
     out->scatter_ms = h->stats.scatter_ms;
+    out->rule = h->stats.rule;
   });
 }
 

@@ -513,9 +513,41 @@ OutColumn make_out(const Allocator& A, cudaStream_t s, int type_id, int64_t rows
 }
 }  // namespace
 
-Result aggregate(const std::vector<Column>& keys, int null_policy, const std::vector<Request>& reqs,
-                 cudaStream_t stream, const Allocator& alloc, const Options& opt, Stats* stats)
+namespace {
+std::mutex g_rules_mu;
+std::vector<TuningRule> g_rules;
+}  // namespace
+
+void set_tuning_rules(const std::vector<TuningRule>& rules)
 {
+  std::lock_guard<std::mutex> lk(g_rules_mu);
+  g_rules = rules;
+}
+
+int apply_tuning_rules(Options& o, int64_t rows, int64_t groups)
+{
+  std::lock_guard<std::mutex> lk(g_rules_mu);
+  for (size_t i = 0; i < g_rules.size(); ++i) {
+    const TuningRule& r = g_rules[i];
+    if (rows > r.max_rows || groups > r.max_groups) continue;
+    const uint32_t m = r.mask & ~o.set_mask;
+    if (m & OPT_BLOCK) o.block = r.opt.block;
+    if (m & OPT_BPS) o.blocks_per_sm = r.opt.blocks_per_sm;
+    if (m & OPT_SMEM) o.smem_bytes = r.opt.smem_bytes;
+    if (m & OPT_FILL) o.smem_fill = r.opt.smem_fill;
+    if (m & OPT_SMEM_MAX) o.smem_max_groups = r.opt.smem_max_groups;
+    if (m & OPT_LOAD) o.load_factor = r.opt.load_factor;
+    if (m & OPT_MODE) o.force_mode = r.opt.force_mode;
+    if (m & OPT_SCATTER) o.scatter = r.opt.scatter;
+    return (int)i;
+  }
+  return -1;
+}
+
+Result aggregate(const std::vector<Column>& keys, int null_policy, const std::vector<Request>& reqs,
+                 cudaStream_t stream, const Allocator& alloc, const Options& opt_in, Stats* stats)
+{
+  Options opt = opt_in;  // tuning rules may adjust it once the group estimate is known
   Plan P;
   std::vector<int> out_types;
   build_plan(keys, null_policy, reqs, P, out_types);
@@ -598,6 +630,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     nsamp = valid_rows;
   }
   st.est_groups = est;
+  st.rule = apply_tuning_rules(opt, n, est);
   mark("estimate");
 
   // ---- mode ----

@@ -78,7 +78,27 @@ struct Options {
   int force_mode = -1;         // -1 auto, 0 global only, 1 smem stage
   int profile = 0;             // time kernels with CUDA events
   int scatter = 0;             // partitioned pass 1 launch shape (0-6: threads x rows per thread)
+  uint32_t set_mask = 0;       // OPT_* bits of the fields a caller set explicitly
 };
+
+// Option fields, as bits of Options::set_mask and TuningRule::mask.
+enum OptBits : uint32_t {
+  OPT_BLOCK = 1, OPT_BPS = 2, OPT_SMEM = 4, OPT_FILL = 8, OPT_SMEM_MAX = 16, OPT_LOAD = 32,
+  OPT_MODE = 64, OPT_SCATTER = 128
+};
+
+// A process-wide tuning rule: for calls with at most max_rows rows and at most
+// max_groups estimated groups, the fields in `mask` take `opt`'s values unless
+// the handle set them itself.  The first matching rule applies.
+struct TuningRule {
+  int64_t max_rows;
+  int64_t max_groups;
+  Options opt;
+  uint32_t mask;
+};
+void set_tuning_rules(const std::vector<TuningRule>& rules);
+// Applies the first rule matching (rows, groups) to `o`; returns its index or -1.
+int apply_tuning_rules(Options& o, int64_t rows, int64_t groups);
 
 struct Stats {
   int64_t est_groups = 0;
@@ -89,6 +109,7 @@ struct Stats {
   double agg_kernel_ms = 0;  // aggregation kernels (partitioned mode: both passes)
   double compact_ms = 0;
   double scatter_ms = 0;     // partitioned mode: pass 1 alone
+  int rule = -1;             // tuning rule applied (-1: none)
 };
 
 // Builds the plan (validates like cudf::groupby::aggregate,

@@ -94,7 +94,7 @@ class GroupBy:
         _lib.check(_lib.lib().gb_get_stats(self._h, ctypes.byref(s)))
         return {"est_groups": s.est_groups, "capacity": s.capacity, "mode": s.mode,
                 "retries": s.retries, "kernels": s.kernels, "agg_kernel_ms": s.agg_kernel_ms,
-                "compact_ms": s.compact_ms, "scatter_ms": s.scatter_ms}
+                "compact_ms": s.compact_ms, "scatter_ms": s.scatter_ms, "rule": s.rule}
 
     def set_profile(self, on: bool = True):
         """Time the aggregation and compaction kernels with CUDA events."""

@@ -154,9 +154,24 @@ typedef struct gb_stats {
   double agg_kernel_ms;     /* device time of the aggregation kernel(s) (profile = 1) */
   double compact_ms;        /* device time of the compaction kernel (profile = 1) */
   double scatter_ms;        /* partitioned mode: device time of the partition pass (profile = 1) */
+  int32_t rule;             /* index of the tuning rule applied, -1 if none */
 } gb_stats;
 
 GB_API int gb_set_tuning(gb_handle* handle, const gb_tuning* tuning);
+
+/* Process-wide tuning by size bucket (no counterpart in libcudf).  Each call
+ * of gb_aggregate, once it has estimated its number of groups, takes the first
+ * rule with rows <= max_rows and groups <= max_groups and applies the rule's
+ * set fields (block, blocks_per_sm, smem_bytes, smem_fill_pct, smem_max_groups,
+ * load_factor_pct, force_mode, scatter) except those its handle set with
+ * gb_set_tuning.  Replaces all rules; NULL/0 clears them.  The rules come
+ * from cudf_b200.autotune, which times the candidates per bucket. */
+typedef struct gb_tuning_rule {
+  int64_t max_rows;
+  int64_t max_groups;
+  gb_tuning tuning;         /* fields < 0 (block, smem_fill_pct, load_factor_pct: <= 0) unset */
+} gb_tuning_rule;
+GB_API int gb_set_tuning_rules(const gb_tuning_rule* rules, int32_t num_rules);
 GB_API int gb_get_stats(const gb_handle* handle, gb_stats* out);
 
 /* Allocation-free groupby.  No counterpart in libcudf: its groupby always

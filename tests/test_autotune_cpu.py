@@ -1,0 +1,33 @@
+"""Tuning rules through the C ABI (host-only calls, no GPU): install, order,
+save/load, and rejection of invalid settings."""
+import json
+
+import pytest
+
+from cudf_b200 import _lib, autotune
+
+
+def test_rules_install_and_clear(tmp_path):
+    rules = [{"max_rows": 1 << 24, "max_groups": 1 << 20, "tuning": {"force_mode": 2, "scatter": 3}},
+             {"max_rows": 1 << 20, "max_groups": 1 << 10, "tuning": {"force_mode": 1, "smem_bytes": 49152}}]
+    ordered = autotune.order_rules(rules)
+    assert [r["max_rows"] for r in ordered] == [1 << 20, 1 << 24]
+    autotune.set_rules(ordered)
+    p = tmp_path / "t.json"
+    autotune.save(ordered, str(p), {"device": "test"})
+    assert json.load(open(p))["rules"] == ordered
+    assert autotune.load(str(p)) == ordered
+    autotune.clear()
+
+
+def test_invalid_rule_is_rejected():
+    with pytest.raises(ValueError):
+        autotune.set_rules([{"max_rows": 10, "max_groups": 10, "tuning": {"scatter": 9}}])
+    with pytest.raises(ValueError):
+        autotune.set_rules([{"max_rows": 10, "max_groups": 10, "tuning": {"force_mode": 5}}])
+    autotune.clear()
+
+
+def test_tuning_struct_defaults_are_unset():
+    t = autotune._tuning_struct({"scatter": 2})
+    assert t.scatter == 2 and t.force_mode == -2 and t.block == -1 and t.smem_bytes == -1

@@ -410,3 +410,26 @@ def test_concurrent_calls_on_separate_streams():
             assert np.array_equal(av[oa], mv[om])
             if avv is not None:
                 assert np.array_equal(avv[oa], mvv[om])
+
+
+def test_tuning_rules_pick_settings_by_size_bucket():
+    """A rule for small calls forces the global table; a larger call falls in
+    the next rule; a handle's own setting wins over the rules."""
+    from cudf_b200 import autotune
+    cb, agg = _cb()
+    rng = np.random.default_rng(39)
+    try:
+        autotune.set_rules([{"max_rows": 300_000, "max_groups": 1 << 30, "tuning": {"force_mode": 0}},
+                            {"max_rows": 1 << 40, "max_groups": 1 << 30, "tuning": {"force_mode": 1}}])
+        for n, want_mode, want_rule in ((200_000, 0, 0), (1_500_000, 1, 1)):
+            k = rng.integers(0, 3000, n).astype(np.int64)
+            v = rng.integers(-10**6, 10**6, n).astype(np.int64)
+            gb, *_ = run_both([cb.Column.from_numpy(k)], [(cb.Column.from_numpy(v), [agg.sum(), agg.max()])])
+            st = gb.stats()
+            assert st["mode"] == want_mode and st["rule"] == want_rule
+        k = rng.integers(0, 3000, 200_000).astype(np.int64)
+        gb, *_ = run_both([cb.Column.from_numpy(k)], [(cb.Column.from_numpy(k), [agg.sum()])],
+                          tuning={"force_mode": 1})
+        assert gb.stats()["mode"] == 1
+    finally:
+        autotune.clear()
