@@ -34,8 +34,9 @@ _UNSET = {"block": -1, "blocks_per_sm": -1, "smem_bytes": -1, "smem_fill_pct": -
 # default buckets: row counts x group counts seen by the benchmark shapes
 DEFAULT_BUCKETS = [
     (1 << 20, 1 << 10), (1 << 20, 1 << 17), (1 << 20, 1 << 20),
-    (1 << 24, 1 << 10), (1 << 24, 1 << 17), (1 << 24, 1 << 22),
-    (1 << 27, 1 << 10), (1 << 27, 1 << 17), (1 << 27, 1 << 20), (1 << 27, 1 << 24),
+    (1 << 24, 1 << 10), (1 << 24, 1 << 17), (1 << 24, 1 << 20), (1 << 24, 1 << 22), (1 << 24, 1 << 24),
+    (1 << 27, 1 << 10), (1 << 27, 1 << 17), (1 << 27, 1 << 20), (1 << 27, 1 << 22), (1 << 27, 1 << 23),
+    (1 << 27, 1 << 24), (1 << 27, 1 << 27),
 ]
 
 # candidate settings per stage of the search (coordinate descent)

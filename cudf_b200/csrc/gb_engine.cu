@@ -645,7 +645,17 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   };
   int scap = smem_cap_for(opt.smem_bytes);
   int sfill = std::max(1, (int)(scap * opt.smem_fill));
-  int64_t smem_max = opt.smem_max_groups >= 0 ? opt.smem_max_groups : 2 * (int64_t)sfill;
+  // groups that outgrow the configured shared-stage table but fit a larger
+  // one (up to ~200 KB at fill 0.7) get the larger one, unless the caller
+  // sized the table
+  if (!(opt.set_mask & (OPT_SMEM | OPT_FILL))) {
+    const int big = smem_cap_for(200 * 1024);
+    if (est > sfill && est <= (int64_t)(0.7 * big)) {
+      scap = big;
+      sfill = std::max(1, (int)(0.7 * big));
+    }
+  }
+  int64_t smem_max = opt.smem_max_groups >= 0 ? opt.smem_max_groups : (int64_t)sfill;
   // partitioned pass 2: as many slots as fit ~220 KB (any count), one more
   // for the all-ones key
   const int scap2 = std::max(0, std::min(220 * 1024, dev.smem_optin - 8192) / P.slot_bytes - 1);
@@ -656,15 +666,21 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     uint8_t op = P.accs[a].op;
     if (op >= OP_PROD_I64 && op <= OP_PROD_F64) part_ok = false;
   }
+  // partitions: enough for ~60% table fill, at most 8192 (the scatter's
+  // per-tile partition arrays take 16 B each in shared memory); beyond
+  // ~85% of that capacity the shared tables would spill most groups and
+  // the global table is faster
+  constexpr int kMaxParts = 8192;
   int nparts = 0;
   if (part_ok) {
     double per = scap2 * 0.6;
-    nparts = (int)std::min<uint64_t>(4096, std::max<uint64_t>(2, next_pow2((uint64_t)std::ceil(est / per))));
+    nparts = (int)std::min<uint64_t>(kMaxParts, std::max<uint64_t>(2, next_pow2((uint64_t)std::ceil(est / per))));
   }
+  const bool part_fits = (double)est <= 0.85 * (double)kMaxParts * sfill2;
   int mode;
   if (opt.force_mode >= 0) mode = opt.force_mode;
   else if (scap >= 64 && est <= smem_max) mode = 1;
-  else if (part_ok && n >= (1 << 20) && est > smem_max) mode = 2;
+  else if (part_ok && part_fits && n >= (1 << 20) && est > smem_max) mode = 2;
   else mode = 0;
   if (mode == 1 && scap < 16) mode = 0;
   if (mode == 2 && !part_ok) mode = 0;
@@ -789,7 +805,10 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     {
       int64_t nrows = 0;
       for (auto r : prows) nrows += r;
-      const int64_t chunk = std::max<int64_t>(nrows / std::max(1, nparts), 32768);
+      // a work item is at most a partition's average share, and small
+      // enough that few partitions still spread over every SM
+      const int64_t chunk = std::max<int64_t>(
+        32768, std::min<int64_t>(nrows / std::max(1, nparts), nrows / (4 * (int64_t)dev.sms)));
       for (int p = 0; p < nparts; ++p) {
         const int64_t r = prows[p];
         if (exact_buckets && r > 2 * chunk) {

@@ -433,3 +433,6 @@ def test_tuning_rules_pick_settings_by_size_bucket():
         assert gb.stats()["mode"] == 1
     finally:
         autotune.clear()
+        import os
+        if os.path.exists(autotune.TUNING_FILE):
+            autotune.load()  # the shipped rules, for the tests that follow
