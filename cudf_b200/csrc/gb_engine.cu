@@ -884,7 +884,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       // rows listed as not fitting their partition's table (none when the
       // sample sized the partitions well): one grid-stride launch that reads
       // the list length on the device
-      k_part_spill<<<dev.sms * 2, 256, 0, stream>>>(P2, G, A);
+      k_part_spill<false><<<dev.sms * 2, 256, 0, stream>>>(P2, G, A);
       k_finish_count<<<1, 1, 0, stream>>>(P, G);
       st.kernels += 3;
       ck(cudaGetLastError(), "partition aggregate launch");
@@ -928,6 +928,23 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     }
   }
 
+  // shared stage through the row-range kernel: plans whose columns all have
+  // closed-form updates and whose groups fit one CTA's ~220 KB table
+  bool raw_stage = mode == 1 && part_ok && opt.block >= 512 && !(opt.set_mask & (OPT_SMEM | OPT_FILL)) &&
+                   est <= (int64_t)(0.7 * sfill2);
+  std::vector<PartItem> raw_items;
+  PartItem* d_raw_items = nullptr;
+  int64_t* d_raw_spill = nullptr;
+  const uint32_t raw_spill_cap = 1u << 16;
+  if (!done && raw_stage) {
+    const int64_t chunk = std::max<int64_t>(32768, (n + 4 * dev.sms - 1) / (4 * dev.sms));
+    for (int64_t b = 0; b < n; b += chunk) raw_items.push_back(PartItem{0, 1, b, std::min(n, b + chunk)});
+    d_raw_items = (PartItem*)S.get(sizeof(PartItem) * raw_items.size());
+    ck(cudaMemcpyAsync(d_raw_items, raw_items.data(), sizeof(PartItem) * raw_items.size(), cudaMemcpyHostToDevice,
+                       stream), "h2d");
+    d_raw_spill = (int64_t*)S.get(sizeof(int64_t) * raw_spill_cap);
+  }
+
   if (!done) {
     for (int attempt = 0;; ++attempt) {
       size_t tbytes = (size_t)(cap + 1) * P.slot_bytes;
@@ -937,7 +954,32 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       G = TableRef{T, cap - 1, P.slot_bytes, P.key_words, counters};
       int block = std::min(opt.block, 512);
       if (opt.profile) ck(cudaEventRecord(events()[0], stream), "event");
-      if (mode == 1) {
+      if (raw_stage) {
+        ck(cudaMemsetAsync(counters + 8, 0, 6 * 4, stream), "memset");  // [8] work, [12..13] spill list
+        PartArgs A;
+        std::memset(&A, 0, sizeof(A));
+        A.counters = counters;
+        A.items = d_raw_items;
+        A.nitems = (int)raw_items.size();
+        A.work = counters + 8;
+        A.spill_rows = d_raw_spill;
+        A.spill_cap = raw_spill_cap;
+        DenseRef D{nullptr, 0, (unsigned long long*)(counters + 10), counters + 6};
+        const size_t sm2 = (size_t)(scap2 + 1) * P.slot_bytes;
+        auto launch_raw = [&](auto kern) {
+          allow_max_smem((const void*)kern);
+          int grid = grid_for((const void*)kern, 1024, sm2, 0);
+          grid = std::min(grid, A.nitems);
+          kern<<<grid, 1024, sm2, stream>>>(P, A, G, D, scap2, sfill2, tmpl);
+        };
+        const bool few = P.num_vals <= 4;
+        if (P.key_words == 1) few ? launch_raw(k_part_aggregate<1, 1, 1024, 4, true, true>)
+                                  : launch_raw(k_part_aggregate<1, 1, 1024, 8, true, true>);
+        else few ? launch_raw(k_part_aggregate<2, 1, 1024, 4, true, true>)
+                 : launch_raw(k_part_aggregate<2, 1, 1024, 8, true, true>);
+        k_part_spill<true><<<dev.sms * 2, 256, 0, stream>>>(P, G, A);
+        st.kernels += 2;
+      } else if (mode == 1) {
         size_t sm = (size_t)scap * P.slot_bytes;
         allow_max_smem((const void*)k_aggregate<true>);
         int grid = grid_for((const void*)k_aggregate<true>, block, sm, opt.blocks_per_sm);
@@ -952,8 +994,13 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       k_finish_count<<<1, 1, 0, stream>>>(P, G);
       st.kernels += 3;
       ck(cudaGetLastError(), "aggregate launch");
-      ck(cudaMemcpyAsync(host, counters, 8, cudaMemcpyDeviceToHost, stream), "count d2h");
+      ck(cudaMemcpyAsync(host, counters, 64, cudaMemcpyDeviceToHost, stream), "count d2h");
       ck(cudaStreamSynchronize(stream), "aggregate sync");
+      if (raw_stage && host[13]) {
+        // more groups than the tables held: redo through the per-row kernel
+        raw_stage = false;
+        host[1] = 1;
+      }
       if (opt.profile) {
         float ms = 0;
         ck(cudaEventElapsedTime(&ms, events()[0], events()[1]), "event time");

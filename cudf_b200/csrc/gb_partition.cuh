@@ -369,8 +369,9 @@ __device__ __forceinline__ uint64_t sld_u64(uint32_t a)
 // loop carries no call into the generic update code.  The list count lives in
 // counters[12]; counters[13] is set when the list itself overflowed (the host
 // then re-runs pass 2 with a longer list).
-static __global__ void __launch_bounds__(256) k_part_spill(const __grid_constant__ Plan P2, TableRef G,
-                                                           const __grid_constant__ PartArgs A)
+template <bool RAW = false>
+__global__ void __launch_bounds__(256) k_part_spill(const __grid_constant__ Plan P2, TableRef G,
+                                                    const __grid_constant__ PartArgs A)
 {
   __shared__ unsigned int s_new;
   if (threadIdx.x == 0) s_new = 0;
@@ -378,8 +379,13 @@ static __global__ void __launch_bounds__(256) k_part_spill(const __grid_constant
   const unsigned cnt = min(*(volatile unsigned int*)(A.counters + 12), A.spill_cap);
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
     const int64_t r = A.spill_rows[i];
-    const uint64_t w0 = P2.packed_keys[r * P2.key_words];
-    const uint64_t w1 = P2.key_words == 2 ? P2.packed_keys[r * 2 + 1] : 0;
+    uint64_t w0, w1;
+    if (RAW) {
+      if (!pack_key(P2, r, w0, w1)) continue;  // not listed: null keys are skipped first
+    } else {
+      w0 = P2.packed_keys[r * P2.key_words];
+      w1 = P2.key_words == 2 ? P2.packed_keys[r * 2 + 1] : 0;
+    }
     const uint64_t h = hash_key(w0, w1, P2.key_words);
     const int64_t gi = global_slot(P2, G, w0, w1, h, &s_new);
     if (gi < 0) {
@@ -614,7 +620,13 @@ __device__ __forceinline__ void p2_column(const ValCol& c, const uint32_t (&sa)[
 // 128-byte line of the key, value and validity arrays), then the columns are
 // applied one at a time, each through code specialised for its type, so the
 // per-type dispatch happens once per column and chunk instead of per row.
-template <int KW, int R, int NT, int MAXV, bool WAGG>
+//
+// With RAW the rows are the caller's own columns (P2 is the plan itself):
+// keys are packed per row, values read at their column offsets and validity
+// taken from the null masks; each item is a row range whose table is merged
+// into the global table.  This is the shared-stage mode for groups that fit
+// one CTA's table.
+template <int KW, int R, int NT, int MAXV, bool WAGG, bool RAW = false>
 __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant__ Plan P2,
                                                           const __grid_constant__ PartArgs A,
                                                           TableRef G, DenseRef D, int scap, int sfill,
@@ -647,16 +659,18 @@ __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant_
       }
       line -= lines;
     };
-    take(P2.packed_keys, 8 * KW);
-    for (int v = 0; v < nv; ++v) take(P2.vals[v].data, P2.vals[v].width);
-    if (have_bits) take(A.bits, 1);
+    if (!RAW) {
+      take(P2.packed_keys, 8 * KW);
+      for (int v = 0; v < nv; ++v) take(P2.vals[v].data, P2.vals[v].width);
+      if (have_bits) take(A.bits, 1);
+    }
   }
   for (;;) {
     const int it = p2_claim<NT>(A, smem, scap + (KW == 1), nw, tmpl, &s_part, &s_used, &s_spill);
     if (it >= A.nitems) break;
     const PartItem item = A.items[it];
     const int64_t b = item.begin;
-    const int64_t e = min(item.end, min((int64_t)A.cursor[item.part], A.end[item.part]));
+    const int64_t e = RAW ? item.end : min(item.end, min((int64_t)A.cursor[item.part], A.end[item.part]));
     auto load_keys = [&](int64_t r0, uint64_t (&k0)[R], uint64_t (&k1)[R], uint32_t (&vb)[R]) {
 #pragma unroll
       for (int j = 0; j < R; ++j) {
@@ -665,13 +679,31 @@ __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant_
         k1[j] = 0;
         vb[j] = 0xFFFFFFFFu;
         if (r < e) {
-          if (KW == 1) k0[j] = __ldg(P2.packed_keys + r);
-          else {
-            const ulonglong2 kk = __ldg((const ulonglong2*)(P2.packed_keys + 2 * r));
-            k0[j] = kk.x;
-            k1[j] = kk.y;
+          if (RAW) {
+            // the caller's columns: a row whose key is null under EXCLUDE
+            // takes no part (vb = 0 marks it); validity bits from the masks
+            uint64_t w0, w1;
+            if (!pack_key(P2, r, w0, w1)) {
+              vb[j] = 0;
+              k0[j] = kEmpty;
+              continue;
+            }
+            k0[j] = w0;
+            k1[j] = w1;
+            uint32_t bits = 0;
+#pragma unroll
+            for (int v = 0; v < MAXV; ++v)
+              if (v < nv && bit_valid(P2.vals[v].mask, r + P2.vals[v].offset)) bits |= 1u << v;
+            vb[j] = bits | 0x80000000u;
+          } else {
+            if (KW == 1) k0[j] = __ldg(P2.packed_keys + r);
+            else {
+              const ulonglong2 kk = __ldg((const ulonglong2*)(P2.packed_keys + 2 * r));
+              k0[j] = kk.x;
+              k1[j] = kk.y;
+            }
+            if (have_bits) vb[j] = __ldg(A.bits + r);
           }
-          if (have_bits) vb[j] = __ldg(A.bits + r);
         }
       }
     };
@@ -692,6 +724,7 @@ __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant_
         row[j] = r0 + (int64_t)j * NT + threadIdx.x;
         sa[j] = 0;
         if (row[j] >= e) continue;
+        if (RAW && vb[j] == 0) continue;  // null key, EXCLUDE
         const uint64_t h = hash_key(k0[j], k1[j], KW);
         uint8_t* slot = (KW == 1 && k0[j] == kEmpty)
                           ? smem + (size_t)scap * stride
@@ -733,7 +766,8 @@ __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant_
 #pragma unroll
         for (int v = 0; v < MAXV; ++v) {
           xv[j][v] = 0;
-          if (v < nv && sa[j] && ((cur_vb[j] >> v) & 1)) xv[j][v] = load_bits(P2.vals[v].data, row[j], P2.vals[v].width);
+          if (v < nv && sa[j] && ((cur_vb[j] >> v) & 1))
+            xv[j][v] = load_bits(P2.vals[v].data, row[j] + (RAW ? P2.vals[v].offset : 0), P2.vals[v].width);
         }
       }
       load_keys(r0 + STEP, k0, k1, vb);
