@@ -56,7 +56,8 @@ class GbStats(ctypes.Structure):
 
 
 class GbTuningRule(ctypes.Structure):
-    _fields_ = [("max_rows", ctypes.c_int64), ("max_groups", ctypes.c_int64), ("tuning", GbTuning)]
+    _fields_ = [("max_rows", ctypes.c_int64), ("max_groups", ctypes.c_int64), ("key_words", ctypes.c_int32),
+                ("tuning", GbTuning)]
 
 
 class GbBatchStats(ctypes.Structure):

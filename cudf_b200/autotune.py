@@ -57,7 +57,8 @@ def set_rules(rules: Sequence[Dict]) -> None:
     in order (the first match applies)."""
     arr = (_lib.GbTuningRule * max(1, len(rules)))()
     for i, r in enumerate(rules):
-        arr[i] = _lib.GbTuningRule(int(r["max_rows"]), int(r["max_groups"]), _tuning_struct(r.get("tuning", {})))
+        arr[i] = _lib.GbTuningRule(int(r["max_rows"]), int(r["max_groups"]), int(r.get("key_words", 0)),
+                                   _tuning_struct(r.get("tuning", {})))
     _lib.check(_lib.lib().gb_set_tuning_rules(arr, len(rules)))
 
 
@@ -160,7 +161,8 @@ def tune(buckets: Sequence[Tuple[int, int]] = DEFAULT_BUCKETS, steps: int = 5, v
     rules, meta = [], {"when": time.strftime("%Y-%m-%dT%H:%M:%S"), "buckets": {}}
     for rows, groups in buckets:
         t, info = tune_bucket(rows, groups, steps, verbose)
-        rules.append({"max_rows": rows, "max_groups": groups, "tuning": t})
+        # tuned on a single 64-bit key: applies to one-word keys only
+        rules.append({"max_rows": rows, "max_groups": groups, "key_words": 1, "tuning": t})
         meta["buckets"][f"{rows}x{groups}"] = info
     return order_rules(rules), meta
 

@@ -198,6 +198,8 @@ int gb_set_tuning_rules(const gb_tuning_rule* rules, int32_t num_rules)
       gb::TuningRule r;
       r.max_rows = rules[i].max_rows;
       r.max_groups = rules[i].max_groups;
+      if (rules[i].key_words < 0 || rules[i].key_words > 2) throw gb::Error(gb::ERR_LOGIC, "key_words must be 0, 1 or 2");
+      r.key_words = rules[i].key_words;
       r.mask = apply_tuning(&rules[i].tuning, r.opt);
       v.push_back(r);
     }

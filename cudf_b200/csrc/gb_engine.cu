@@ -524,12 +524,12 @@ void set_tuning_rules(const std::vector<TuningRule>& rules)
   g_rules = rules;
 }
 
-int apply_tuning_rules(Options& o, int64_t rows, int64_t groups)
+int apply_tuning_rules(Options& o, int64_t rows, int64_t groups, int key_words)
 {
   std::lock_guard<std::mutex> lk(g_rules_mu);
   for (size_t i = 0; i < g_rules.size(); ++i) {
     const TuningRule& r = g_rules[i];
-    if (rows > r.max_rows || groups > r.max_groups) continue;
+    if (rows > r.max_rows || groups > r.max_groups || (r.key_words && r.key_words != key_words)) continue;
     const uint32_t m = r.mask & ~o.set_mask;
     if (m & OPT_BLOCK) o.block = r.opt.block;
     if (m & OPT_BPS) o.blocks_per_sm = r.opt.blocks_per_sm;
@@ -630,7 +630,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     nsamp = valid_rows;
   }
   st.est_groups = est;
-  st.rule = apply_tuning_rules(opt, n, est);
+  st.rule = apply_tuning_rules(opt, n, est, P.key_words);
   mark("estimate");
 
   // ---- mode ----
@@ -937,7 +937,10 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   int64_t* d_raw_spill = nullptr;
   const uint32_t raw_spill_cap = 1u << 16;
   if (!done && raw_stage) {
-    const int64_t chunk = std::max<int64_t>(32768, (n + 4 * dev.sms - 1) / (4 * dev.sms));
+    // one row range per CTA for small inputs (each range pays a table reset
+    // and a merge), four per SM for large ones
+    const int64_t per_cta = (n + dev.sms - 1) / dev.sms;
+    const int64_t chunk = per_cta < 4 * 32768 ? per_cta : std::max<int64_t>(32768, (n + 4 * dev.sms - 1) / (4 * dev.sms));
     for (int64_t b = 0; b < n; b += chunk) raw_items.push_back(PartItem{0, 1, b, std::min(n, b + chunk)});
     d_raw_items = (PartItem*)S.get(sizeof(PartItem) * raw_items.size());
     ck(cudaMemcpyAsync(d_raw_items, raw_items.data(), sizeof(PartItem) * raw_items.size(), cudaMemcpyHostToDevice,

@@ -93,12 +93,13 @@ enum OptBits : uint32_t {
 struct TuningRule {
   int64_t max_rows;
   int64_t max_groups;
+  int key_words;  // 0 any, else the packed key width the rule was tuned for
   Options opt;
   uint32_t mask;
 };
 void set_tuning_rules(const std::vector<TuningRule>& rules);
 // Applies the first rule matching (rows, groups) to `o`; returns its index or -1.
-int apply_tuning_rules(Options& o, int64_t rows, int64_t groups);
+int apply_tuning_rules(Options& o, int64_t rows, int64_t groups, int key_words);
 
 struct Stats {
   int64_t est_groups = 0;

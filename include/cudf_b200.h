@@ -161,7 +161,8 @@ GB_API int gb_set_tuning(gb_handle* handle, const gb_tuning* tuning);
 
 /* Process-wide tuning by size bucket (no counterpart in libcudf).  Each call
  * of gb_aggregate, once it has estimated its number of groups, takes the first
- * rule with rows <= max_rows and groups <= max_groups and applies the rule's
+ * rule with rows <= max_rows, groups <= max_groups and a matching key width,
+ * and applies the rule's
  * set fields (block, blocks_per_sm, smem_bytes, smem_fill_pct, smem_max_groups,
  * load_factor_pct, force_mode, scatter) except those its handle set with
  * gb_set_tuning.  Replaces all rules; NULL/0 clears them.  The rules come
@@ -169,6 +170,8 @@ GB_API int gb_set_tuning(gb_handle* handle, const gb_tuning* tuning);
 typedef struct gb_tuning_rule {
   int64_t max_rows;
   int64_t max_groups;
+  int32_t key_words;        /* 1 or 2: only calls whose keys pack into that many 64-bit
+                               words (single 64-bit key: 1); 0: any */
   gb_tuning tuning;         /* fields < 0 (block, smem_fill_pct, load_factor_pct: <= 0) unset */
 } gb_tuning_rule;
 GB_API int gb_set_tuning_rules(const gb_tuning_rule* rules, int32_t num_rules);
