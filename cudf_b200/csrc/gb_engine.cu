@@ -666,14 +666,14 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     uint8_t op = P.accs[a].op;
     if (op >= OP_PROD_I64 && op <= OP_PROD_F64) part_ok = false;
   }
-  // partitions: enough for ~60% table fill, at most 8192 (the scatter's
+  // partitions: enough for ~70% table fill, at most 8192 (the scatter's
   // per-tile partition arrays take 16 B each in shared memory); beyond
   // ~85% of that capacity the shared tables would spill most groups and
   // the global table is faster
   constexpr int kMaxParts = 8192;
   int nparts = 0;
   if (part_ok) {
-    double per = scap2 * 0.6;
+    double per = scap2 * 0.7;
     nparts = (int)std::min<uint64_t>(kMaxParts, std::max<uint64_t>(2, next_pow2((uint64_t)std::ceil(est / per))));
   }
   const bool part_fits = (double)est <= 0.85 * (double)kMaxParts * sfill2;
