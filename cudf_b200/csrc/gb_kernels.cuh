@@ -7,7 +7,8 @@
 //   k_var_pass       second pass of VARIANCE/STD
 //   k_finish_count   adds the all-ones-key slot to the group count
 //   k_compact        gathers occupied slots into dense key and result columns
-//   k_sample*        key sample for the group-count estimate
+//   k_sketch         full-pass HyperLogLog + per-bucket row counts (group
+//                    estimate, partition region sizes)
 #pragma once
 #include <cub/block/block_scan.cuh>
 
@@ -394,30 +395,10 @@ static __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ 
     compact_block(P, T, nslots, stride, limit, dense, O, base, &tmp, &s_base);
 }
 
-// ---- group-count estimate from a key sample ----
-// Sample slots: key words (16 B) + u32 count at byte 16; stride 32.
-// Also counts sampled keys per hash bucket (top kBucketBits bits of the hash)
-// so the partitioned path can size its regions.
+// ---- group-count estimate ----
+// Hash buckets (top kBucketBits bits of a key's hash) of the sketch's row
+// histogram; the partitioned path sizes its regions from them.
 constexpr int kBucketBits = 14;
-static __global__ void __launch_bounds__(256) k_sample(const __grid_constant__ Plan P, TableRef S, int64_t nsamp,
-                                                unsigned int* buckets)
-{
-  const int64_t n = P.num_rows;
-  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nsamp;
-       j += (int64_t)gridDim.x * blockDim.x) {
-    int64_t row = nsamp >= n ? j : (int64_t)(((__int128)j * n) / nsamp);
-    uint64_t w0, w1;
-    if (!pack_key(P, row, w0, w1)) continue;
-    uint64_t h = hash_key(w0, w1, P.key_words);
-    atomicAdd(buckets + (h >> (64 - kBucketBits)), 1u);
-    bool ins;
-    int64_t gi = P.key_words == 1 ? find_or_insert1(S.T, S.stride, S.cap_mask, w0, h, (int)(S.cap_mask + 1), ins)
-                                  : find_or_insert2(S.T, S.stride, S.cap_mask, w0, w1, h, (int)(S.cap_mask + 1), ins);
-    if (gi < 0) { atomicOr(S.counters + 1, 1u); continue; }
-    atomicAdd((unsigned int*)(S.T + gi * (int64_t)S.stride + 16), 1u);
-    atomicAdd(S.counters + 3, 1u);  // sampled rows that take part
-  }
-}
 
 // Full-pass key sketch: per hash bucket (top kBucketBits bits) the exact
 // number of rows with a valid key, and a HyperLogLog register array
@@ -470,19 +451,5 @@ static __global__ void __launch_bounds__(512) k_sketch(const __grid_constant__ P
     if (bk[i]) atomicAdd(buckets + i, bk[i]);
 }
 
-// counters: [4] distinct, [5] seen once, [6] seen twice
-static __global__ void __launch_bounds__(256) k_sample_stats(const __grid_constant__ Plan P, TableRef S)
-{
-  int64_t nslots = (int64_t)S.cap_mask + 2;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nslots;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const uint8_t* slot = S.T + i * (int64_t)S.stride;
-    uint32_t c = *(const uint32_t*)(slot + 16);
-    bool occ = c > 0;
-    count_nulls(occ, S.counters + 4);
-    count_nulls(c == 1, S.counters + 5);
-    count_nulls(c == 2, S.counters + 6);
-  }
-}
 
 }  // namespace gb

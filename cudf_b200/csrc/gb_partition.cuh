@@ -9,10 +9,17 @@
 //                     hash as partition id, and scatter key words, value bits
 //                     and a validity byte into that partition's region.  One
 //                     global atomic per (tile, partition) reserves space.
-//   k_part_aggregate  pass 2: one CTA at a time owns a partition and
+//   k_part_aggregate  pass 2: one CTA at a time owns a work item -- a
+//                     partition, or a row range of a heavy partition -- and
 //                     aggregates it in a shared-memory table; its groups are
 //                     then copied out as dense slots (or merged into a global
-//                     spill table when the partition did not fit).
+//                     spill table for split partitions and partitions that did
+//                     not fit).  Items of split partitions combine the rows of
+//                     one slot per warp before the shared update.  The same
+//                     kernel over row ranges of the caller's own columns is
+//                     the shared-stage mode for groups that fit one CTA.
+//   k_part_spill      applies the rows listed as not fitting their table to
+//                     the global spill table.
 #pragma once
 #include <cub/block/block_scan.cuh>
 
