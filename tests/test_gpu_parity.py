@@ -436,3 +436,48 @@ def test_tuning_rules_pick_settings_by_size_bucket():
         import os
         if os.path.exists(autotune.TUNING_FILE):
             autotune.load()  # the shipped rules, for the tests that follow
+
+
+@pytest.mark.parametrize("policy", [False, True])
+def test_shared_stage_row_ranges_match_both_kernels(policy):
+    """Low cardinality: the row-range kernel (closed-form plans, warp-combined
+    updates) and the per-row shared-stage kernel (taken when the caller sizes
+    the table) both equal the oracle, on sliced columns with nullable keys."""
+    cb, agg = _cb()
+    rng = np.random.default_rng(40)
+    n = 1_200_000
+    off = 37
+    k1 = rng.integers(0, 4, n + off).astype(np.int32)           # a few hot keys
+    k2 = rng.integers(0, 60, n + off).astype(np.int64)
+    kv = rng.random(n + off) > 0.05
+    cols = [(rng.integers(-2**40, 2**40, n + off).astype(np.int64), rng.random(n + off) > 0.1),
+            (rng.normal(size=n + off).astype(np.float32), rng.random(n + off) > 0.1),
+            (rng.integers(0, 2**16, n + off).astype(np.uint16), None)]
+
+    def sliced(arr, valid, tid=None):
+        c = cb.Column.from_numpy(arr, valid, tid) if tid is not None else cb.Column.from_numpy(arr, valid)
+        return cb.Column(c.type_id, c.data, c.mask, size=n, offset=off)
+
+    keys = [sliced(k1, kv), sliced(k2, None)]
+    aggs = [agg.sum(), agg.min(), agg.max(), agg.count(), agg.mean(), agg.sum_of_squares()]
+    reqs = [(sliced(v, m), aggs) for v, m in cols]
+    gb, *_ = run_both(keys, reqs, include_null_keys=policy)
+    assert gb.stats()["mode"] == 1
+    gb, *_ = run_both(keys, reqs, include_null_keys=policy, tuning={"smem_bytes": 200_000, "smem_fill_pct": 70})
+    assert gb.stats()["mode"] == 1
+
+
+def test_partitioned_many_partitions_wide_slots():
+    """Wide slots (eight value columns) leave ~1000 slots per shared table, so
+    3.5M groups need 8192 partitions; every group and value must still match."""
+    cb, agg = _cb()
+    rng = np.random.default_rng(41)
+    n = 4_000_000
+    key = rng.integers(0, 3_500_000, n).astype(np.int64) * 1_000_003
+    reqs = []
+    for i in range(8):
+        v = rng.integers(-10**9, 10**9, n).astype(np.int64)
+        reqs.append((cb.Column.from_numpy(v, rng.random(n) > 0.1 if i % 2 else None),
+                     [agg.sum(), agg.min(), agg.max()]))
+    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs)
+    assert gb.stats()["mode"] == 2
