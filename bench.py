@@ -326,9 +326,21 @@ def run_engine(args):
 
     def compute(b):
         nonlocal d2h
-        uk2, res2 = cb.GroupBy(cb.Table([bufs[b][1]])).aggregate(bufs[b][2], stream=stream)
-        outs = [c.values() for c in uk2.columns] + [c.values() for t in res2 for c in t.columns]
-        outs += [c.mask for t in res2 for c in t.columns if c.mask is not None]
+        if world > 1:
+            # the whole multi-GPU call: partial aggregate, exchange, merge
+            from cudf_b200.distributed import distributed_groupby
+            from cudf_b200.types import Kind
+            kinds = [Kind.SUM, Kind.COUNT_VALID, Kind.MIN, Kind.MAX, Kind.MEAN]
+            t = bufs[b][0]
+            types = (TypeId.INT64, TypeId.FLOAT64, TypeId.FLOAT32)
+            mk, mres = distributed_groupby(
+                [(t[0], None, TypeId.INT64)],
+                [((t[1 + i], cb.column.unpack_mask(t[4 + i], n), types[i]), kinds) for i in range(3)])
+            outs = [d for d, _, _ in mk] + [x for per in mres for pair in per for x in pair if x is not None]
+        else:
+            uk2, res2 = cb.GroupBy(cb.Table([bufs[b][1]])).aggregate(bufs[b][2], stream=stream)
+            outs = [c.values() for c in uk2.columns] + [c.values() for t in res2 for c in t.columns]
+            outs += [c.mask for t in res2 for c in t.columns if c.mask is not None]
         host = staging.to_host(outs, stream)
         d2h = sum(h.nbytes for h in host)
         return host
