@@ -778,7 +778,10 @@ __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant_
         }
       }
       load_keys(r0 + STEP, k0, k1, vb);
-#pragma unroll
+      // one copy of the per-type column code, looped over the columns (the
+      // values are picked from registers by predicated moves), keeps the
+      // kernel small enough for the instruction cache
+#pragma unroll 1
       for (int v = 0; v < MAXV; ++v) {
         if (v >= nv) break;
         const ValCol& c = P2.vals[v];
