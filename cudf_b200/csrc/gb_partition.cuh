@@ -215,7 +215,16 @@ __global__ void __launch_bounds__(NT, MINB) k_part_scatter(const __grid_constant
         x[k] = pr[k] != 0xFFFFFFFFu ? load_bits(c.data, t0 + i + c.offset, c.width) : 0;
       }
     };
-    if (PF && nv > 0) load_col(0);
+    // a column of at most 4 bytes shares its round with the validity bytes
+    // (value at +0 and validity at +4 of an 8-byte stage slot), saving the
+    // validity bytes' own round; it goes last, once every column's validity
+    // bit is known
+    int vn = -1;
+    if (any_bits)
+      for (int v = 0; v < nv; ++v)
+        if (P.vals[v].width <= 4) vn = v;
+    auto col_at = [&](int vi) { return vn < 0 || vi < vn ? vi : (vi == nv - 1 ? vn : vi + 1); };
+    if (PF && nv > 0) load_col(col_at(0));
     __syncthreads();
     for (int s = threadIdx.x; s < nvalid; s += NT) {
       const unsigned p = psort[s];
@@ -240,7 +249,8 @@ __global__ void __launch_bounds__(NT, MINB) k_part_scatter(const __grid_constant
 #pragma unroll
     for (int k = 0; k < (RPT + 3) / 4; ++k) vb[k] = 0;
 #pragma unroll 1
-    for (int v = 0; v < nv; ++v) {
+    for (int vi = 0; vi < nv; ++vi) {
+      const int v = col_at(vi);
       const ValCol& c = P.vals[v];
       if (any_bits) {
 #pragma unroll
@@ -250,12 +260,33 @@ __global__ void __launch_bounds__(NT, MINB) k_part_scatter(const __grid_constant
       }
       if (!PF) load_col(v);
       __syncthreads();  // the previous write-out has read the stage
+      void* dst = A.vals[v];
+      if (v == vn) {
+#pragma unroll
+        for (int k = 0; k < RPT; ++k)
+          if (pr[k] != 0xFFFFFFFFu) {
+            const unsigned s = pr[k] & 0xFFFFu;
+            ((uint32_t*)stage)[2 * s] = (uint32_t)x[k];
+            stage[8 * s + 4] = (uint8_t)(vb[k >> 2] >> (8 * (k & 3)));
+          }
+        __syncthreads();
+        for (int s = threadIdx.x; s < nvalid; s += NT) {
+          const unsigned p = psort[s];
+          if ((unsigned)s >= send[p]) continue;
+          const int64_t g = delta[p] + s;
+          const uint32_t w = ((const uint32_t*)stage)[2 * s];
+          if (c.width == 4) ((uint32_t*)dst)[g] = w;
+          else if (c.width == 2) ((uint16_t*)dst)[g] = (uint16_t)w;
+          else ((uint8_t*)dst)[g] = (uint8_t)w;
+          A.bits[g] = stage[8 * s + 4];
+        }
+        continue;
+      }
 #pragma unroll
       for (int k = 0; k < RPT; ++k)
         if (pr[k] != 0xFFFFFFFFu) store_width(stage, pr[k] & 0xFFFFu, c.width, x[k]);
       __syncthreads();
-      if (PF && v + 1 < nv) load_col(v + 1);
-      void* dst = A.vals[v];
+      if (PF && vi + 1 < nv) load_col(col_at(vi + 1));
       switch (c.width) {
         case 8:
           for (int s = threadIdx.x; s < nvalid; s += NT) {
@@ -283,7 +314,7 @@ __global__ void __launch_bounds__(NT, MINB) k_part_scatter(const __grid_constant
           break;
       }
     }
-    if (any_bits) {
+    if (any_bits && vn < 0) {
       __syncthreads();
 #pragma unroll
       for (int k = 0; k < RPT; ++k)
