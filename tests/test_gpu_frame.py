@@ -110,3 +110,21 @@ def test_arrow_table_groupby():
     assert out.column("k").to_pylist() == [1, 2, None]
     assert out.column(1).to_pylist() == [7.0, 7.0, 4.0]
     assert out.column(2).to_pylist() == [2, 2, 1]
+
+
+def test_host_staging_round_trips_and_reuses_buffers():
+    """HostStaging copies device results into reused pinned buffers; each call's
+    arrays hold that call's data."""
+    import torch
+    import cudf_b200 as cb
+    st = cb.HostStaging()
+    for seed in (1, 2):
+        g = torch.Generator(device="cuda")
+        g.manual_seed(seed)
+        ts = [torch.randint(-2**40, 2**40, (1000,), device="cuda", generator=g, dtype=torch.int64),
+              torch.rand(777, device="cuda", generator=g, dtype=torch.float32),
+              torch.rand(33, device="cuda", generator=g) > 0.5,
+              torch.empty(0, device="cuda", dtype=torch.float64)]
+        out = st.to_host(ts)
+        for t, h in zip(ts, out):
+            assert h.dtype == t.cpu().numpy().dtype and np.array_equal(h, t.cpu().numpy())
