@@ -12,8 +12,12 @@ Prints one JSON line (rank 0).  `value` is rows/s of the whole aggregate() call
 with inputs resident in HBM (device-timed with CUDA events, max over ranks);
 `e2e` is the same call through the public API with pinned host inputs copied
 in and results copied out inside the timed region.  `--impl reference` times
-the CPU restatement of the reference algorithm (oracle/) on the host cores on a
-bounded sample of the same workload.
+the CPU restatement of the reference algorithm (oracle/) on the host cores, one
+full pass over the same 100M-row workload per step.  At one GPU the line also
+carries `extra`: the Zipf two-key, 1M-row, batched and serving workloads,
+measured after the main one (`--no-extra` skips them).  `--check` compares the
+last timed call's result with the oracle on the same inputs, group by group,
+after the timed region.
 """
 from __future__ import annotations
 
@@ -36,7 +40,7 @@ SEED = 1
 NULL_FRAC = 0.10
 AGG_NAMES = ["sum", "count", "min", "max", "mean"]
 METRIC = "groupby rows/s (100M rows, 1M groups, 3 value cols, sum/count/min/max/mean)"
-CPU_SAMPLE_ROWS = 8_000_000
+CPU_SAMPLE_ROWS = N_ROWS
 
 # Kernels whose device time the roofline covers, by engine mode (0 global
 # table, 1 shared-memory stage, 2 hash-partitioned two-pass).
@@ -62,6 +66,19 @@ def algorithmic_bytes(n_rows: int, n_groups: int) -> tuple[float, float]:
     # keys 8; per value col: sum, count(4), min, max, mean(8) + masks for sum/min/max/mean
     out = n_groups * 8 + n_groups * (8 + 4 + 8 + 8 + 8) * 2 + n_groups * (4 + 4 + 4 + 4 + 8) + 3 * 4 * gmask
     return float(inp), float(out)
+
+
+WORKLOAD = ("groupby 100M rows, int64 key over 1M distinct values, v1 int64, v2 f64, v3 f32, "
+            "10% nulls, sum/count/min/max/mean")
+
+
+def workload_config(rows_per_rank: int, world: int, groups: int) -> dict:
+    """The `config` object of both arms (engine and reference)."""
+    return {"workload": WORKLOAD, "rows": rows_per_rank * world, "rows_per_rank": rows_per_rank,
+            "groups": groups,
+            "parallelism": (f"rows sharded over {world} ranks, partial aggregate + NCCL all-to-all by key "
+                            f"owner + merge") if world > 1 else "single",
+            "l2": "inputs (2.84 GB) larger than L2 (126 MB); no flush needed"}
 
 
 def make_inputs_host(n: int, seed: int = SEED):
@@ -175,19 +192,31 @@ def dist_setup():
     return world, rank, local
 
 
-def cpu_reference(n_sample: int, threads: int):
-    """The oracle (CPU restatement of the reference algorithm) on a sample."""
+def _oracle_inputs(key, vals, masks):
     from oracle import oracle as O
-    key, vals, masks = make_inputs_host(n_sample)
     kinds = [O.SUM, O.COUNT_VALID, O.MIN, O.MAX, O.MEAN]
     kc = O.HostColumn(O.INT64, key)
     reqs = [(O.HostColumn(O.INT64, vals[0], masks[0]), kinds),
             (O.HostColumn(O.FLOAT64, vals[1], masks[1]), kinds),
             (O.HostColumn(O.FLOAT32, vals[2], masks[2]), kinds)]
-    O.groupby([kc], reqs, nthreads=threads)  # warm
+    return [kc], reqs
+
+
+def cpu_reference(n_rows: int, threads: int, steps: int = 1, warmup: int = 1):
+    """The oracle (CPU restatement of the reference algorithm) over n_rows rows of
+    the workload's distributions, `warmup` untimed and `steps` timed full passes.
+    Returns (rows/s over the timed passes, seconds per pass, groups)."""
+    from oracle import oracle as O
+    key, vals, masks = make_inputs_host(n_rows)
+    keys, reqs = _oracle_inputs(key, vals, masks)
+    r = None
+    for _ in range(warmup):
+        r = O.groupby(keys, reqs, nthreads=threads)
     t = time.perf_counter()
-    O.groupby([kc], reqs, nthreads=threads)
-    return n_sample / (time.perf_counter() - t)
+    for _ in range(steps):
+        r = O.groupby(keys, reqs, nthreads=threads)
+    dt = (time.perf_counter() - t) / max(1, steps)
+    return n_rows / dt, dt, r.num_groups
 
 
 def run_reference(args):
@@ -196,24 +225,34 @@ def run_reference(args):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    n_sample = CPU_SAMPLE_ROWS
-    vals = []
-    for _ in range(max(1, args.steps)):
-        vals.append(cpu_reference(n_sample, threads))
-    v = float(np.median(vals))
+    n = args.rows
+    v, sec, groups = cpu_reference(n, threads, steps=max(1, args.steps), warmup=args.warmup)
     line = {"metric": METRIC, "value": v, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": N_ROWS / v * 1e3, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64/f32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "groupby 100M rows, int64 key over 1M distinct values, v1 int64, "
-                                   "v2 f64, v3 f32, 10% nulls, sum/count/min/max/mean", "rows": N_ROWS,
-                       "groups": N_DISTINCT, "parallelism": f"replicas{world}"},
+            "config": workload_config(n, 1, groups),
             "cpu_baseline": {"value": v, "unit": "rows/s", "cores": threads, "kind": "port",
-                             "sample": f"{n_sample} rows with the workload's distributions (numpy seed 1, "
-                                       f"1M distinct keys), oracle/gb_oracle.c with {threads} threads"},
+                             "sample": f"every step one full pass over {n} rows with the workload's "
+                                       f"distributions (numpy seed 1, 1M distinct keys), oracle/gb_oracle.c "
+                                       f"(rows hash-partitioned by key, partitions aggregated in parallel) "
+                                       f"with {threads} threads"},
             "e2e": {"value": v, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def check_with_oracle(host_keys, host_reqs, include_null_keys, uk, res):
+    """Compares an engine result with the oracle on the same host inputs, group by
+    group after sorting by key: integer results bit-exact, float SUM/MEAN within
+    the oracle's per-group bound.  Raises AssertionError on a mismatch."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import parity
+    from oracle import oracle as O
+    o = O.groupby(host_keys, host_reqs, include_null_keys=include_null_keys, nthreads=os.cpu_count() or 1)
+    parity.compare(o, parity.gpu_pairs(uk), [parity.gpu_pairs(t) for t in res],
+                   [list(kinds) for _, kinds in host_reqs], None)
+    return o.num_groups
 
 
 def run_engine(args):
@@ -295,6 +334,16 @@ def run_engine(args):
         t = torch.tensor([ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
+    checked = None
+    if args.check and world == 1:
+        # outside the timed region: the last timed call's groups against the
+        # oracle on the same inputs
+        t0 = time.perf_counter()
+        hk, hr = _oracle_inputs(key.cpu().numpy(), [v.cpu().numpy() for v in vals],
+                                [cb.column.unpack_mask(m, n).cpu().numpy() for m in masks])
+        g = check_with_oracle(hk, hr, False, uk, res)
+        checked = {"groups": g, "result": "match", "seconds": round(time.perf_counter() - t0, 1)}
+        del hk, hr
     del uk, res
 
     # ---- e2e through the public API from pinned host buffers ----
@@ -397,7 +446,9 @@ def run_engine(args):
         inp, outb = algorithmic_bytes(n, groups)
         kmean = float(np.mean(kernel_ms)) if kernel_ms else float("nan")
         smean = float(np.mean(scatter_ms)) if scatter_ms else 0.0
-        achieved = inp / (kmean * 1e-3) / 1e9
+        # every input read once plus every output written once, over the
+        # device time of the dominant kernels of one call
+        achieved = (inp + outb) / (kmean * 1e-3) / 1e9
         mode = last_stats.get("mode", -1)
         kname = KERNELS_BY_MODE.get(mode, "unknown")
         tm = TRAFFIC_MODEL.get(mode)
@@ -407,18 +458,15 @@ def run_engine(args):
             "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64/f64/f32", "data": "synthetic",
-            "config": {"workload": "groupby 100M rows, int64 key over 1M distinct values, v1 int64, "
-                                   "v2 f64, v3 f32, 10% nulls, sum/count/min/max/mean",
-                       "rows": n * world, "rows_per_rank": n, "groups": groups,
-                       "parallelism": f"rows sharded over {world} ranks, partial aggregate + NCCL all-to-all by key owner + merge" if world > 1 else "single",
-                       "l2": "inputs (2.84 GB) larger than L2 (126 MB); no flush needed"},
+            "config": workload_config(n, world, groups),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": kname,
                          "kernel_ms": kmean, "kernel_ms_steps": [round(x, 3) for x in kernel_ms],
                          "kernel_split_ms": {"partition_scatter": smean,
                                                                  "partition_aggregate": kmean - smean}
                          if mode == 2 else None,
-                         "algorithmic_bytes": inp, "peak_source": peak_src,
+                         "algorithmic_bytes": inp + outb, "input_bytes": inp, "output_bytes": outb,
+                         "peak_source": peak_src,
                          "traffic_source": TRAFFIC_SOURCE.get(mode),
                          "whole_call_frac": (inp + outb) / (ms * 1e-3) / 1e9 / peak},
             "e2e": {"value": world * n / (e_ms * 1e-3), "unit": "rows/s", "h2d_bytes_per_step": h2d,
@@ -430,12 +478,20 @@ def run_engine(args):
             "engine": last_stats,
             "clocks": clk.summary(),
         }
+        if checked is not None:
+            line["check"] = checked
         if not args.no_cpu_baseline and world == 1:
             threads = os.cpu_count() or 1
-            v = cpu_reference(args.cpu_sample, threads)
+            v, _, _ = cpu_reference(args.cpu_sample, threads)
             line["cpu_baseline"] = {"value": v, "unit": "rows/s", "cores": threads, "kind": "port",
-                                    "sample": f"{args.cpu_sample} rows with the workload's distributions (numpy seed 1, "
-                                              f"1M distinct keys) through oracle/gb_oracle.c, {threads} threads"}
+                                    "sample": f"one full pass over {args.cpu_sample} rows with the workload's "
+                                              f"distributions (numpy seed 1, 1M distinct keys) through "
+                                              f"oracle/gb_oracle.c, {threads} threads"}
+        if not args.no_extra and world == 1:
+            bufs.clear()
+            hosts.clear()
+            torch.cuda.empty_cache()
+            line["extra"] = run_extras(args)
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
@@ -513,8 +569,7 @@ def run_batch(args):
             "batched": {"ms_per_pass": batch_ms, "rows_per_s": total_rows / (batch_ms * 1e-3),
                         "prepare_ms": prepare_ms, **st},
             "speedup_vs_plain": plain_ms / batch_ms}
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def run_serve(args):
@@ -624,8 +679,59 @@ def run_serve(args):
             "batched": b, "plain": p, "plain_single_query_latency_s": alone_p50,
             "qps_ratio_vs_plain": b["queries_per_s"] / p["queries_per_s"],
             "p99_over_plain_single": b["p99_s"] / alone_p50}
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
+
+
+def zipf_inputs_device(n: int, dev):
+    """Zipf two-key workload on the device (seed 2): k1 int32, k2 int64,
+    packed key masks (5% nulls each), v_int int64 [0, 1e6], v_f f64 [0, 1)."""
+    import torch
+    from cudf_b200.column import pack_mask
+    g = torch.Generator(device=dev)
+    g.manual_seed(2)
+    p = _zipf_pairs(n, dev, g)
+    k1 = (p // 1000).to(torch.int32)
+    k2 = p % 1000
+    del p
+    km = [pack_mask(torch.rand(n, device=dev, generator=g) >= 0.05) for _ in range(2)]
+    vi = torch.randint(0, 10**6 + 1, (n,), device=dev, generator=g, dtype=torch.int64)
+    vf = torch.rand(n, device=dev, generator=g, dtype=torch.float64)
+    return k1, k2, km, vi, vf
+
+
+def small_inputs_device(n: int, dev):
+    """1M-row workload on the device (seed 0): int32 key over 1000 values,
+    v1 int64 [0, 1e6], v2 f64 [0, 1), no nulls."""
+    import torch
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    k = torch.randint(0, 1000, (n,), device=dev, generator=g, dtype=torch.int32)
+    v1 = torch.randint(0, 10**6 + 1, (n,), device=dev, generator=g, dtype=torch.int64)
+    v2 = torch.rand(n, device=dev, generator=g, dtype=torch.float64)
+    return k, v1, v2
+
+
+def _flat(cols):
+    out = []
+    for c in cols:
+        out.extend(c if isinstance(c, (list, tuple)) else [c])
+    return out
+
+
+def config_oracle_inputs(workload, host, n):
+    """Oracle columns for the zipf/small workloads from host copies of the
+    device inputs (in the order of `_flat`)."""
+    from oracle import oracle as O
+    if workload == "zipf":
+        k1, k2, m1, m2, vi, vf = [t.numpy() for t in host]
+        kinds = [O.SUM, O.COUNT_VALID, O.MAX]
+        keys = [O.HostColumn(O.INT32, k1, packed=m1.view(np.uint32)),
+                O.HostColumn(O.INT64, k2, packed=m2.view(np.uint32))]
+        return keys, [(O.HostColumn(O.INT64, vi), kinds), (O.HostColumn(O.FLOAT64, vf), kinds)], True
+    k, v1, v2 = [t.numpy() for t in host]
+    return ([O.HostColumn(O.INT32, k)],
+            [(O.HostColumn(O.INT64, v1), [O.SUM, O.COUNT_VALID, O.MIN, O.MAX]),
+             (O.HostColumn(O.FLOAT64, v2), [O.MEAN])], False)
 
 
 def _zipf_pairs(n, dev, g, s=1.1, support=50_000_000):
@@ -657,17 +763,10 @@ def run_config(args):
     from cudf_b200.types import NullPolicy, TypeId
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    g = torch.Generator(device=dev)
     if args.workload == "zipf":
         n = args.rows if args.rows != N_ROWS else 100_000_000
-        g.manual_seed(2)
-        p = _zipf_pairs(n, dev, g)
-        k1 = (p // 1000).to(torch.int32)
-        k2 = p % 1000
-        del p
-        km = [pack_mask(torch.rand(n, device=dev, generator=g) >= 0.05) for _ in range(2)]
-        vi = torch.randint(0, 10**6 + 1, (n,), device=dev, generator=g, dtype=torch.int64)
-        vf = torch.rand(n, device=dev, generator=g, dtype=torch.float64)
+        cols = zipf_inputs_device(n, dev)
+        k1, k2, km, vi, vf = cols
         keys = cb.Table([cb.Column(TypeId.INT32, k1, km[0]), cb.Column(TypeId.INT64, k2, km[1])])
         aggs = [agg.sum(), agg.count(), agg.max()]
         reqs = [cb.GroupByRequest(cb.Column(TypeId.INT64, vi), aggs), cb.GroupByRequest(cb.Column(TypeId.FLOAT64, vf), aggs)]
@@ -675,18 +774,18 @@ def run_config(args):
         workload = ("groupby 100M rows, (int32, int64) keys = divmod(Zipf(1.1) on [0,50M), 1000), 5% key nulls, "
                     "INCLUDE, int64 + f64 values, sum/count/max")
         inp = n * (4 + 8 + 8 + 8) + 2 * ((n + 31) // 32) * 4
+        out_per_group, out_masks = 4 + 8 + 8 + 4 + 8 + 8 + 4 + 8, 2
     else:
         n = args.rows if args.rows != N_ROWS else 1_000_000
-        g.manual_seed(0)
-        k = torch.randint(0, 1000, (n,), device=dev, generator=g, dtype=torch.int32)
-        v1 = torch.randint(0, 10**6 + 1, (n,), device=dev, generator=g, dtype=torch.int64)
-        v2 = torch.rand(n, device=dev, generator=g, dtype=torch.float64)
+        cols = small_inputs_device(n, dev)
+        k, v1, v2 = cols
         keys = cb.Table([cb.Column(TypeId.INT32, k)])
         reqs = [cb.GroupByRequest(cb.Column(TypeId.INT64, v1), [agg.sum(), agg.count(), agg.min(), agg.max()]),
                 cb.GroupByRequest(cb.Column(TypeId.FLOAT64, v2), [agg.mean()])]
         policy = NullPolicy.EXCLUDE
         workload = "groupby 1M rows, int32 key over 1000 values, v1 int64 sum/count/min/max, v2 f64 mean"
         inp = n * (4 + 8 + 8)
+        out_per_group, out_masks = 4 + 8 + 4 + 8 + 8 + 8, 0
     torch.cuda.synchronize()
     gb = cb.GroupBy(keys, policy)
     gb.set_profile(True)
@@ -706,6 +805,14 @@ def run_config(args):
     ms = a.elapsed_time(b) / args.steps
     st = gb.stats()
     groups = uk.num_rows()
+    checked = None
+    if args.check:
+        t0 = time.perf_counter()
+        hk, hr, inc = config_oracle_inputs(args.workload, [c.cpu() for c in _flat(cols)], n)
+        g = check_with_oracle(hk, hr, inc, uk, res)
+        checked = {"groups": g, "result": "match", "seconds": round(time.perf_counter() - t0, 1)}
+        del hk, hr
+    algo = inp + groups * out_per_group + out_masks * ((groups + 31) // 32) * 4
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -717,15 +824,17 @@ def run_config(args):
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/int64/f64",
             "data": "synthetic", "config": {"workload": workload, "rows": n, "groups": groups},
-            "roofline": {"bound": "hbm", "achieved": inp / (kmean * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
-                         "frac": inp / (kmean * 1e-3) / 1e9 / peak, "traffic": None,
+            "roofline": {"bound": "hbm", "achieved": algo / (kmean * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": algo / (kmean * 1e-3) / 1e9 / peak, "traffic": None,
                          "kernel": KERNELS_BY_MODE.get(st["mode"]), "kernel_ms": kmean,
-                         "algorithmic_bytes": inp},
+                         "algorithmic_bytes": algo, "input_bytes": inp,
+                         "whole_call_frac": algo / (ms * 1e-3) / 1e9 / peak},
             "engine": st, "clocks": clk.summary()}
+    if checked is not None:
+        line["check"] = checked
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = _cpu_config(args.workload, min(n, args.cpu_sample))
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def _cpu_config(workload, n):
@@ -756,6 +865,40 @@ def _cpu_config(workload, n):
             "sample": f"{n} rows with the workload's distributions through oracle/gb_oracle.c, {threads} threads"}
 
 
+def run_extras(args) -> dict:
+    """The other workloads, each measured once after the main one (shorter runs
+    than their own --workload lines; each entry says what it ran)."""
+    import copy
+    import torch
+    out = {}
+
+    def one(name, fn, **kw):
+        a = copy.copy(args)
+        for k, v in kw.items():
+            setattr(a, k, v)
+        try:
+            r = fn(a)
+        except Exception as e:  # one failing workload leaves the others
+            r = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        return r
+
+    z = one("zipf", run_config, workload="zipf", rows=N_ROWS, steps=5, warmup=2, no_cpu_baseline=True)
+    out["zipf"] = {k: z.get(k) for k in ("metric", "value", "unit", "ms_per_step", "config", "roofline", "error")
+                   if k in z}
+    sm = one("small", run_config, workload="small", rows=N_ROWS, steps=50, warmup=5, no_cpu_baseline=True)
+    out["small"] = {k: sm.get(k) for k in ("metric", "value", "unit", "ms_per_step", "config", "error") if k in sm}
+    b = one("batch", run_batch, steps=3, warmup=2)
+    out["batch"] = {k: b.get(k) for k in ("metric", "value", "unit", "ms_per_step", "config", "plain",
+                                          "speedup_vs_plain", "error") if k in b}
+    sv = one("serve", run_serve, duration=args.serve_duration)
+    out["serve"] = {k: sv.get(k) for k in ("metric", "value", "unit", "config", "batched", "plain",
+                                           "plain_single_query_latency_s", "qps_ratio_vs_plain",
+                                           "p99_over_plain_single", "error") if k in sv}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -774,13 +917,16 @@ def main():
     ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--direct-rows", type=int, default=0,
                     help="serve: queries with at least this many rows run alone (0: server default)")
+    ap.add_argument("--check", action="store_true",
+                    help="compare the last timed result with the oracle on the same inputs")
+    ap.add_argument("--no-extra", action="store_true", help="skip the other workloads in the main line")
+    ap.add_argument("--serve-duration", type=float, default=5.0,
+                    help="length of the serving stream measured in the main line's extra")
     args = ap.parse_args()
-    if args.workload == "batch" and args.impl == "engine":
-        return run_batch(args)
-    if args.workload == "serve" and args.impl == "engine":
-        return run_serve(args)
-    if args.workload in ("zipf", "small") and args.impl == "engine":
-        return run_config(args)
+    if args.impl == "engine" and args.workload in ("batch", "serve", "zipf", "small"):
+        fn = {"batch": run_batch, "serve": run_serve}.get(args.workload, run_config)
+        print(json.dumps(fn(args)), flush=True)
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run_engine(args)

@@ -64,5 +64,30 @@ def build(verbose: bool = False, force: bool = False) -> str:
     return LIB
 
 
+CPP_TESTS = os.path.join(ROOT, "tests", "cpp")
+CPP_TEST_BIN = os.path.join(OUT, "groupby_api_golden")
+
+
+def build_cpp_tests() -> str:
+    """Compiles the C++ program that drives the engine through
+    include/cudf_b200/groupby.hpp (libcudf's groupby API shapes), linked
+    against the in-tree library; used by tests/test_gpu_cpp_api.py."""
+    lib = build()
+    src = os.path.join(CPP_TESTS, "groupby_api_golden.cpp")
+    hdrs = [os.path.join(ROOT, "include", "cudf_b200", "groupby.hpp"), os.path.join(ROOT, "include", "cudf_b200.h")]
+    if (os.path.exists(CPP_TEST_BIN) and all(os.path.getmtime(CPP_TEST_BIN) > os.path.getmtime(f)
+                                             for f in [src, lib, *hdrs])):
+        return CPP_TEST_BIN
+    cuda = os.path.dirname(os.path.dirname(NVCC))
+    cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(cuda, "include"), src, "-o", CPP_TEST_BIN, "-L", OUT, "-lcudf_b200",
+           "-L", os.path.join(cuda, "lib64"), "-lcudart", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"C++ API test build failed:\n{r.stdout}\n{r.stderr}")
+    return CPP_TEST_BIN
+
+
 if __name__ == "__main__":
     print(build(verbose="--verbose" in sys.argv, force="--force" in sys.argv))
+    print(build_cpp_tests())

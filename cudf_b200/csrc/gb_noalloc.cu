@@ -12,10 +12,12 @@
 // The array is static __device__ memory of this module, so every GPU that loads
 // the library holds GB_NOALLOC_SCRATCH_BYTES of it until the process exits.  In
 // host code the array's name is only a host-side stand-in, not a device
-// address: its device address is looked up once per device with
+// address: its device address is looked up once per device (and again if the
+// device's context was recreated, e.g. after cudaDeviceReset) with
 // cudaGetSymbolAddress, with that device current.  That lookup happens on the
 // first call on each device, so the first call on a device should come before
-// any stream capture.  Every call shares the one array and leaves its contents
+// any stream capture.  The call is synchronous: it waits for its stream and
+// returns with the results complete.  Every call shares the one array and leaves its contents
 // behind; each call clears the counters (and the caller's null masks) it relies
 // on before use.  Calls that overlap on the GPU -- on different streams, or
 // from different threads -- race on the array and must be serialised by the
@@ -33,17 +35,39 @@ namespace {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[GB_NOALLOC_SCRATCH_BYTES];
 
-// Device address of g_noalloc_scratch on the current device (looked up once).
+// The current CUDA context (driver entry point fetched through the runtime,
+// so the library needs no link-time dependency on libcuda).
+void* current_context()
+{
+  using get_ctx_fn = int (*)(void**);
+  static get_ctx_fn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<get_ctx_fn>(f);
+  }();
+  void* ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
+
+// Device address of g_noalloc_scratch on the current device.  It is looked up
+// once per device and context: a context made after cudaDeviceReset has the
+// array at a new address, so a change of context repeats the lookup.
 void* scratch_address()
 {
   static std::mutex mu;
   static void* addr[64] = {};
+  static void* ctx_of[64] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) throw gb::Error(gb::ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= 64) throw gb::Error(gb::ERR_UNSUPPORTED, "device ordinal out of range");
   std::lock_guard<std::mutex> g(mu);
-  if (!addr[dev]) {
+  void* ctx = current_context();
+  if (!addr[dev] || ctx_of[dev] != ctx || !ctx) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
@@ -51,6 +75,7 @@ void* scratch_address()
       throw gb::Error(gb::ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     }
     addr[dev] = p;
+    ctx_of[dev] = current_context();
   }
   return addr[dev];
 }

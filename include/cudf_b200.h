@@ -195,7 +195,10 @@ GB_API int gb_get_stats(const gb_handle* handle, gb_stats* out);
  *    plus 4 KiB of counters; larger requests are rejected with GB_ERR_LOGIC,
  *    and so is a groupby that finds more than max_groups groups.
  *  - the first call on a device looks up the array's device address
- *    (cudaGetSymbolAddress); make that call before any stream capture.
+ *    (cudaGetSymbolAddress; again if the device's context was recreated);
+ *    make that call before any stream capture.
+ *  - the call is synchronous: it waits for its stream and returns with the
+ *    results complete.
  *  - all calls share the array: calls that overlap on the GPU race and must be
  *    serialised by the caller. */
 #define GB_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)

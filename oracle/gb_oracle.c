@@ -38,8 +38,9 @@
  * leaves this order-dependent; cpp/tests/groupby/min_tests.cpp:524-547 only
  * pins that it terminates).
  *
- * Groups are reported in first-appearance order.  The reference's order is
- * arbitrary (cpp/include/cudf/groupby.hpp:153-155); callers sort by key.
+ * One thread reports groups in first-appearance order; several threads report
+ * them partition by partition (see groupby_parallel).  The reference's order
+ * is arbitrary (cpp/include/cudf/groupby.hpp:153-155); callers sort by key.
  */
 #include <math.h>
 #include <pthread.h>
@@ -443,65 +444,16 @@ static void update_row(acc_t* a, const orc_column* v, int64_t g, int64_t row)
   }
 }
 
-static void aggregate_range(orc_handle* h, int64_t lo, int64_t hi)
+/* Aggregates rows idx[0..cnt) (or rows lo..lo+cnt when idx is NULL) in order. */
+static void aggregate_rows(orc_handle* h, const int64_t* idx, int64_t lo, int64_t cnt)
 {
   uint64_t kw[65];
-  for (int64_t row = lo; row < hi; ++row) {
+  for (int64_t i = 0; i < cnt; ++i) {
+    const int64_t row = idx ? idx[i] : lo + i;
     if (row_key(h, row, kw)) continue;
     int64_t g = find_or_insert(h, kw, row);
     for (int r = 0; r < h->nreq; ++r) update_row(&h->acc[r], &h->reqs[r].values, g, row);
   }
-}
-
-/* merge group gs of src into group gd of dst (chunks are merged in row order) */
-static void merge_group(acc_t* d, const acc_t* s, int64_t gd, int64_t gs, const orc_column* v)
-{
-  d->n_all[gd] += s->n_all[gs];
-  d->n_valid[gd] += s->n_valid[gs];
-  if (d->isum) d->isum[gd] += s->isum[gs];
-  if (d->fsum) { neumaier(&d->fsum[gd], &d->fcomp[gd], s->fsum[gs]); d->fcomp[gd] += s->fcomp[gs]; d->fabs_sum[gd] += s->fabs_sum[gs]; }
-  if (d->iprod) d->iprod[gd] *= s->iprod[gs];
-  if (d->fprod) d->fprod[gd] *= s->fprod[gs];
-  if (d->imin && s->imin[gs] < d->imin[gd]) d->imin[gd] = s->imin[gs];
-  if (d->imax && s->imax[gs] > d->imax[gd]) d->imax[gd] = s->imax[gs];
-  if (d->umin && s->umin[gs] < d->umin[gd]) d->umin[gd] = s->umin[gs];
-  if (d->umax && s->umax[gs] > d->umax[gd]) d->umax[gd] = s->umax[gs];
-  if (d->fmin && s->fmin_seen[gs]) {
-    double x = s->fmin[gs];
-    if (!d->fmin_seen[gd] || x < d->fmin[gd]) d->fmin[gd] = x;
-    d->fmin_seen[gd] = 1;
-  }
-  if (d->fmax && s->fmax_seen[gs]) {
-    double x = s->fmax[gs];
-    if (!d->fmax_seen[gd] || x > d->fmax[gd]) d->fmax[gd] = x;
-    d->fmax_seen[gd] = 1;
-  }
-  if (d->isq) d->isq[gd] += s->isq[gs];
-  if (d->fsq) { neumaier(&d->fsq[gd], &d->fsq_comp[gd], s->fsq[gs]); d->fsq_comp[gd] += s->fsq_comp[gs]; }
-  if (d->argmin) {
-    int64_t a = d->argmin[gd], b = s->argmin[gs];
-    if (a < 0) d->argmin[gd] = b;
-    else if (b >= 0) {
-      if (d->cat == C_FLOAT) { double x = load_float(v, b), y = load_float(v, a); if (x < y || (isnan(y) && !isnan(x))) d->argmin[gd] = b; }
-      else if (d->cat == C_UNSIGNED) { if (load_unsigned(v, b) < load_unsigned(v, a)) d->argmin[gd] = b; }
-      else if (load_signed(v, b) < load_signed(v, a)) d->argmin[gd] = b;
-    }
-    a = d->argmax[gd]; b = s->argmax[gs];
-    if (a < 0) d->argmax[gd] = b;
-    else if (b >= 0) {
-      if (d->cat == C_FLOAT) { double x = load_float(v, b), y = load_float(v, a); if (x > y || (isnan(y) && !isnan(x))) d->argmax[gd] = b; }
-      else if (d->cat == C_UNSIGNED) { if (load_unsigned(v, b) > load_unsigned(v, a)) d->argmax[gd] = b; }
-      else if (load_signed(v, b) > load_signed(v, a)) d->argmax[gd] = b;
-    }
-  }
-}
-
-typedef struct { orc_handle* h; int64_t lo, hi; } job_t;
-static void* run_job(void* p)
-{
-  job_t* j = (job_t*)p;
-  aggregate_range(j->h, j->lo, j->hi);
-  return NULL;
 }
 
 /* mean of group g in double, as the second pass sees it (sum of the target type / count) */
@@ -513,13 +465,14 @@ static double group_mean(const acc_t* a, int64_t g)
   return s / (double)a->n_valid[g];
 }
 
-static void second_pass_var(orc_handle* h)
+static void second_pass_var(orc_handle* h, const int64_t* idx, int64_t lo, int64_t cnt)
 {
   uint64_t kw[65];
   int any = 0;
   for (int r = 0; r < h->nreq; ++r) any |= h->acc[r].need_var;
   if (!any) return;
-  for (int64_t row = 0; row < h->keys[0].size; ++row) {
+  for (int64_t i = 0; i < cnt; ++i) {
+    const int64_t row = idx ? idx[i] : lo + i;
     if (row_key(h, row, kw)) continue;
     uint64_t s = hash_words(kw, h->nkw) & (uint64_t)(h->tcap - 1);
     int64_t g;
@@ -540,6 +493,162 @@ static void second_pass_var(orc_handle* h)
   }
 }
 
+/* ---- parallel path -------------------------------------------------------
+ * Rows are hash-partitioned by their normalised key tuple, so every group lives
+ * in exactly one partition; each partition is then aggregated on its own in
+ * increasing row order.  A group therefore sees its rows in the same order as
+ * in the single-threaded path (identical float sums, first rows and argmin/
+ * argmax ties), and the partitions' groups are concatenated.  Only the order of
+ * the groups differs, which the reference leaves arbitrary. */
+#define ORC_PART_BITS 10
+#define ORC_NPART (1 << ORC_PART_BITS)
+#define ORC_SKIP 0xFFFFu
+
+typedef struct {
+  orc_handle* proto;       /* keys, requests, policy */
+  int nthreads;
+  int64_t n;
+  uint16_t* pid;           /* partition of each row, ORC_SKIP when dropped */
+  int64_t* counts;         /* [nthreads][ORC_NPART], then running offsets */
+  int64_t* idx;            /* rows grouped by partition */
+  int64_t part_start[ORC_NPART + 1];
+  orc_handle* parts[ORC_NPART];
+  int next;                /* next partition to aggregate (atomic) */
+} par_t;
+
+typedef struct { par_t* p; int t; } par_job;
+
+static void* par_count(void* arg)
+{
+  par_job* j = (par_job*)arg;
+  par_t* p = j->p;
+  orc_handle* h = p->proto;
+  const int64_t lo = p->n * j->t / p->nthreads, hi = p->n * (j->t + 1) / p->nthreads;
+  int64_t* cnt = p->counts + (int64_t)j->t * ORC_NPART;
+  uint64_t kw[65];
+  for (int64_t row = lo; row < hi; ++row) {
+    if (row_key(h, row, kw)) { p->pid[row] = ORC_SKIP; continue; }
+    const unsigned q = (unsigned)(hash_words(kw, h->nkw) >> (64 - ORC_PART_BITS));
+    p->pid[row] = (uint16_t)q;
+    cnt[q]++;
+  }
+  return NULL;
+}
+
+static void* par_scatter(void* arg)
+{
+  par_job* j = (par_job*)arg;
+  par_t* p = j->p;
+  const int64_t lo = p->n * j->t / p->nthreads, hi = p->n * (j->t + 1) / p->nthreads;
+  int64_t* off = p->counts + (int64_t)j->t * ORC_NPART;
+  for (int64_t row = lo; row < hi; ++row) {
+    const unsigned q = p->pid[row];
+    if (q != ORC_SKIP) p->idx[off[q]++] = row;
+  }
+  return NULL;
+}
+
+static void* par_aggregate(void* arg)
+{
+  par_job* j = (par_job*)arg;
+  par_t* p = j->p;
+  orc_handle* pr = p->proto;
+  for (;;) {
+    const int q = __atomic_fetch_add(&p->next, 1, __ATOMIC_RELAXED);
+    if (q >= ORC_NPART) break;
+    const int64_t b = p->part_start[q], cnt = p->part_start[q + 1] - b;
+    orc_handle* h = handle_new(pr->keys, pr->nkeys, pr->include_nulls, pr->reqs, pr->nreq);
+    aggregate_rows(h, p->idx + b, 0, cnt);
+    second_pass_var(h, p->idx + b, 0, cnt);
+    p->parts[q] = h;
+  }
+  return NULL;
+}
+
+static void run_threads(par_t* p, void* (*fn)(void*))
+{
+  pthread_t th[256];
+  par_job jobs[256];
+  for (int t = 0; t < p->nthreads; ++t) {
+    jobs[t].p = p;
+    jobs[t].t = t;
+    pthread_create(&th[t], NULL, fn, &jobs[t]);
+  }
+  for (int t = 0; t < p->nthreads; ++t) pthread_join(th[t], NULL);
+}
+
+/* Appends the accumulators of groups [0, n) of s at position at of d
+ * (d's arrays are allocated for at least at + n groups). */
+#define CAT(field, T)                                                                  \
+  do {                                                                                 \
+    if (d->field) memcpy(d->field + at, s->field, (size_t)n * sizeof(T));              \
+  } while (0)
+static void acc_append(acc_t* d, const acc_t* s, int64_t at, int64_t n)
+{
+  CAT(n_all, int64_t); CAT(n_valid, int64_t); CAT(isum, uint64_t); CAT(fsum, double);
+  CAT(fcomp, double); CAT(fabs_sum, double); CAT(iprod, uint64_t); CAT(fprod, long double);
+  CAT(imin, int64_t); CAT(imax, int64_t); CAT(umin, uint64_t); CAT(umax, uint64_t);
+  CAT(fmin, double); CAT(fmax, double); CAT(fmin_seen, uint8_t); CAT(fmax_seen, uint8_t);
+  CAT(isq, uint64_t); CAT(fsq, double); CAT(fsq_comp, double); CAT(argmin, int64_t);
+  CAT(argmax, int64_t); CAT(m2, long double);
+}
+#undef CAT
+
+static orc_handle* groupby_parallel(const orc_column* keys, int nkeys, int include_null_keys,
+                                    const orc_request* reqs, int nreq, int nthreads, int64_t n)
+{
+  par_t* p = xcalloc(1, sizeof(par_t));
+  p->proto = handle_new(keys, nkeys, include_null_keys, reqs, nreq);
+  p->nthreads = nthreads;
+  p->n = n;
+  p->pid = xcalloc(n, sizeof(uint16_t));
+  p->counts = xcalloc((int64_t)nthreads * ORC_NPART, sizeof(int64_t));
+  run_threads(p, par_count);
+  /* partition-major offsets: partition q's rows from thread 0, then 1, ... */
+  int64_t total = 0;
+  for (int q = 0; q < ORC_NPART; ++q) {
+    p->part_start[q] = total;
+    for (int t = 0; t < nthreads; ++t) {
+      int64_t c = p->counts[(int64_t)t * ORC_NPART + q];
+      p->counts[(int64_t)t * ORC_NPART + q] = total;
+      total += c;
+    }
+  }
+  p->part_start[ORC_NPART] = total;
+  p->idx = xcalloc(total, sizeof(int64_t));
+  run_threads(p, par_scatter);
+  free(p->pid);
+  p->pid = NULL;
+  run_threads(p, par_aggregate);
+  free(p->idx);
+  free(p->counts);
+  /* concatenate the partitions' groups */
+  int64_t G = 0;
+  for (int q = 0; q < ORC_NPART; ++q) G += p->parts[q]->ngroups;
+  orc_handle* h = p->proto;
+  if (G > h->gcap) {
+    h->gkeys = xrealloc(h->gkeys, G * h->nkw, 8);
+    h->first_row = xrealloc(h->first_row, G, 8);
+    for (int r = 0; r < nreq; ++r) acc_grow(&h->acc[r], h->gcap, G);
+    h->gcap = G;
+  }
+  int64_t at = 0;
+  for (int q = 0; q < ORC_NPART; ++q) {
+    orc_handle* s = p->parts[q];
+    const int64_t m = s->ngroups;
+    if (m) {
+      memcpy(h->gkeys + at * h->nkw, s->gkeys, (size_t)(m * h->nkw) * 8);
+      memcpy(h->first_row + at, s->first_row, (size_t)m * 8);
+      for (int r = 0; r < nreq; ++r) acc_append(&h->acc[r], &s->acc[r], at, m);
+    }
+    at += m;
+    handle_free(s);
+  }
+  h->ngroups = G;
+  free(p);
+  return h;
+}
+
 int orc_groupby(const orc_column* keys, int nkeys, int include_null_keys,
                 const orc_request* reqs, int nreq, int nthreads, orc_handle** out)
 {
@@ -557,32 +666,13 @@ int orc_groupby(const orc_column* keys, int nkeys, int include_null_keys,
   if (nthreads < 1) nthreads = 1;
   if (n < 65536) nthreads = 1;
   if (nthreads > 256) nthreads = 256;
-  orc_handle* hs[256];
-  job_t jobs[256];
-  pthread_t th[256];
-  for (int t = 0; t < nthreads; ++t) {
-    hs[t] = handle_new(keys, nkeys, include_null_keys, reqs, nreq);
-    jobs[t].h = hs[t];
-    jobs[t].lo = n * t / nthreads;
-    jobs[t].hi = n * (t + 1) / nthreads;
+  if (nthreads > 1) {
+    *out = groupby_parallel(keys, nkeys, include_null_keys, reqs, nreq, nthreads, n);
+    return 0;
   }
-  if (nthreads == 1) run_job(&jobs[0]);
-  else {
-    for (int t = 0; t < nthreads; ++t) pthread_create(&th[t], NULL, run_job, &jobs[t]);
-    for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
-  }
-  orc_handle* h = hs[0];
-  for (int t = 1; t < nthreads; ++t) {
-    orc_handle* s = hs[t];
-    for (int64_t gs = 0; gs < s->ngroups; ++gs) {
-      int64_t before = h->ngroups;
-      int64_t gd = find_or_insert(h, &s->gkeys[gs * s->nkw], s->first_row[gs]);
-      (void)before;
-      for (int r = 0; r < nreq; ++r) merge_group(&h->acc[r], &s->acc[r], gd, gs, &reqs[r].values);
-    }
-    handle_free(s);
-  }
-  second_pass_var(h);
+  orc_handle* h = handle_new(keys, nkeys, include_null_keys, reqs, nreq);
+  aggregate_rows(h, NULL, 0, n);
+  second_pass_var(h, NULL, 0, n);
   *out = h;
   return 0;
 }

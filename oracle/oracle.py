@@ -82,18 +82,34 @@ def unpack_mask(words: np.ndarray, n: int) -> np.ndarray:
 
 @dataclass
 class HostColumn:
+    """``valid`` (bool per row) or ``packed`` (libcudf validity words) may be
+    given; a column built from words unpacks them only if its validity is read
+    as bools (key columns)."""
     type_id: int
     data: np.ndarray
     valid: Optional[np.ndarray] = None
+    packed: Optional[np.ndarray] = None
 
     def __post_init__(self):
         self.data = np.ascontiguousarray(self.data, dtype=NP_DTYPE[self.type_id])
+        self._words = None
+        if self.packed is not None:
+            self._words = np.ascontiguousarray(self.packed, dtype=np.uint32)
+            assert self._words.size >= (self.data.shape[0] + 31) // 32
+            if self.valid is None:
+                self.valid = unpack_mask(self._words, self.data.shape[0])
         if self.valid is not None:
             self.valid = np.ascontiguousarray(self.valid, dtype=bool)
             assert self.valid.shape == self.data.shape
 
     def __len__(self):
         return self.data.shape[0]
+
+    def words(self) -> Optional[np.ndarray]:
+        """The validity as packed words, computed once per column."""
+        if self._words is None and self.valid is not None:
+            self._words = pack_mask(self.valid)
+        return self._words
 
 
 class _Col(ctypes.Structure):
@@ -140,7 +156,7 @@ def lib():
 
 @dataclass
 class OracleResult:
-    group_rows: np.ndarray            # first row of each group (first-appearance order)
+    group_rows: np.ndarray            # first row of each group
     keys: list                        # [(data, valid)] per key column
     results: list                     # results[r][j] = (values, valid, tol)
 
@@ -160,14 +176,14 @@ def groupby(keys: Sequence[HostColumn], requests: Sequence[tuple], include_null_
     keep = []
     kcols = (_Col * len(keys))()
     for i, k in enumerate(keys):
-        m = pack_mask(k.valid)
+        m = k.words()
         keep.append(m)
         kcols[i] = _Col(k.type_id, len(k), k.data.ctypes.data, 0 if m is None else m.ctypes.data, 0)
     reqs = (_Req * max(1, len(requests)))()
     for i, rq in enumerate(requests):
         col, kinds = rq[0], list(rq[1])
         ddof = list(rq[2]) if len(rq) > 2 and rq[2] is not None else [1] * len(kinds)
-        m = pack_mask(col.valid)
+        m = col.words()
         ka = np.asarray(kinds, dtype=np.int32)
         da = np.asarray(ddof, dtype=np.int32)
         keep += [m, ka, da]

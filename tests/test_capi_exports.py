@@ -54,3 +54,31 @@ def test_invalid_arguments_are_reported_not_thrown():
     col = _lib.GbColumn(3, 4, 0, 0, 0)
     rc = L.gb_create(ctypes.byref(col), 1, 7, 0, ctypes.byref(h))
     assert rc == _lib.GB_ERR_LOGIC
+
+
+def test_cpp_api_header_compiles_standalone():
+    """include/cudf_b200/groupby.hpp (libcudf's groupby API shapes over the C
+    ABI) compiles on its own with warnings as errors, and a caller written
+    against libcudf's signatures type-checks against it."""
+    import subprocess
+    import tempfile
+    src = r'''
+#include <cudf_b200/groupby.hpp>
+int use(cudf::table_view const& keys, cudf::column_view const& vals) {
+  cudf::groupby::groupby gb(keys, cudf::null_policy::INCLUDE, cudf::sorted::NO);
+  std::vector<cudf::groupby::aggregation_request> reqs(1);
+  reqs[0].values = vals;
+  reqs[0].aggregations.push_back(cudf::make_sum_aggregation<cudf::groupby_aggregation>());
+  reqs[0].aggregations.push_back(cudf::make_mean_aggregation<cudf::groupby_aggregation>());
+  reqs[0].aggregations.push_back(cudf::make_count_aggregation<cudf::groupby_aggregation>(cudf::null_policy::INCLUDE));
+  auto [uk, res] = gb.aggregate(reqs, cudf::get_default_stream(), rmm::mr::get_current_device_resource());
+  return uk->num_rows() + static_cast<int>(res[0].results.size());
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        f = os.path.join(d, "use.cpp")
+        open(f, "w").write(src)
+        r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only",
+                            "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include", f],
+                           capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
