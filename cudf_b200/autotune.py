@@ -29,7 +29,8 @@ TUNING_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning_b
 
 # fields of a rule's tuning, with the value meaning "unset" in gb_tuning
 _UNSET = {"block": -1, "blocks_per_sm": -1, "smem_bytes": -1, "smem_fill_pct": -1, "smem_max_groups": -1,
-          "load_factor_pct": -1, "force_mode": -2, "groups_hint": -1, "profile": -1, "scatter": -1}
+          "load_factor_pct": -1, "force_mode": -2, "groups_hint": -1, "profile": -1, "scatter": -1,
+          "pass2": -1}
 
 # default buckets: row counts x group counts seen by the benchmark shapes
 DEFAULT_BUCKETS = [

@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT, "libcudf_b200.so")
 
-SOURCES = ["gb_engine.cu", "gb_capi.cu", "gb_noalloc.cu", "gb_batch.cu", "gb_server.cu"]
+SOURCES = ["gb_engine.cu", "gb_sorted.cu", "gb_scatter.cu", "gb_capi.cu", "gb_noalloc.cu", "gb_batch.cu", "gb_server.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",

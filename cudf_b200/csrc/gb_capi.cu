@@ -174,9 +174,14 @@ static uint32_t apply_tuning(const gb_tuning* t, gb::Options& o)
   if (t->groups_hint >= 0) o.groups_hint = t->groups_hint;
   if (t->profile >= 0) o.profile = t->profile;
   if (t->scatter >= 0) {
-    if (t->scatter > 6) throw gb::Error(gb::ERR_LOGIC, "scatter must be in [0, 6]");
+    if (t->scatter > 7) throw gb::Error(gb::ERR_LOGIC, "scatter must be in [0, 7]");
     o.scatter = t->scatter;
     m |= gb::OPT_SCATTER;
+  }
+  if (t->pass2 >= 0) {
+    if (t->pass2 > 3) throw gb::Error(gb::ERR_LOGIC, "pass2 must be in [0, 3]");
+    o.pass2 = t->pass2;
+    m |= gb::OPT_PASS2;
   }
   return m;
 }

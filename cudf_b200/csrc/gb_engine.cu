@@ -16,6 +16,8 @@
 #include "gb_engine.h"
 #include "gb_kernels.cuh"
 #include "gb_partition.cuh"
+#include "gb_scatter.h"
+#include "gb_sorted.h"
 
 namespace gb {
 
@@ -117,6 +119,8 @@ struct Scratch {
     void* p = A.allocate(A.ctx, n, (void*)s);
     if (!p) throw Error(ERR_ALLOC, "device allocation of " + std::to_string(n) + " bytes failed");
     bufs.push_back({p, n});
+    // kernels read scratch arrays with 16-byte vector loads and bulk copies
+    if ((uintptr_t)p & 15) throw Error(ERR_LOGIC, "the allocator returned a block that is not 16-byte aligned");
     return p;
   }
   void put(void* p)
@@ -485,15 +489,6 @@ double hll_estimate(const std::vector<uint32_t>& regs)
   return e;
 }
 
-int grid_for(const void* kernel, int block, size_t smem, int bps_cap)
-{
-  DevInfo d = dev_info();
-  int bps = 0;
-  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, block, smem), "occupancy");
-  if (bps < 1) bps = 1;
-  if (bps_cap > 0) bps = std::min(bps, bps_cap);
-  return d.sms * bps;
-}
 
 OutColumn make_out(const Allocator& A, cudaStream_t s, int type_id, int64_t rows, bool nullable)
 {
@@ -512,6 +507,16 @@ OutColumn make_out(const Allocator& A, cudaStream_t s, int type_id, int64_t rows
   return c;
 }
 }  // namespace
+
+int grid_for(const void* kernel, int block, size_t smem, int bps_cap)
+{
+  DevInfo d = dev_info();
+  int bps = 0;
+  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, block, smem), "occupancy");
+  if (bps < 1) bps = 1;
+  if (bps_cap > 0) bps = std::min(bps, bps_cap);
+  return d.sms * bps;
+}
 
 namespace {
 std::mutex g_rules_mu;
@@ -539,6 +544,7 @@ int apply_tuning_rules(Options& o, int64_t rows, int64_t groups, int key_words)
     if (m & OPT_LOAD) o.load_factor = r.opt.load_factor;
     if (m & OPT_MODE) o.force_mode = r.opt.force_mode;
     if (m & OPT_SCATTER) o.scatter = r.opt.scatter;
+    if (m & OPT_PASS2) o.pass2 = r.opt.pass2;
     return (int)i;
   }
   return -1;
@@ -656,9 +662,24 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     }
   }
   int64_t smem_max = opt.smem_max_groups >= 0 ? opt.smem_max_groups : (int64_t)sfill;
-  // partitioned pass 2: as many slots as fit ~220 KB (any count), one more
-  // for the all-ones key
-  const int scap2 = std::max(0, std::min(220 * 1024, dev.smem_optin - 8192) / P.slot_bytes - 1);
+  // partitioned pass 2.  Per-row variant: as many slots as fit ~220 KB (any
+  // count), one more for the all-ones key.  Sorted-chunk variants: the slots
+  // that fit beside the chunk's sorted stage and the two per-slot count arrays.
+  bool any_val_null = false;
+  for (int v = 0; v < P.num_vals; ++v) any_val_null |= P.vals[v].mask != nullptr;
+  const bool p2_sorted = opt.pass2 != 1;
+  const int p2_rows = part_sorted_rows(opt.pass2, P.num_vals);  // rows per sorted chunk
+  int scap2;
+  if (p2_sorted) {
+    const size_t budget = (size_t)std::min(227 * 1024, dev.smem_optin) - 4096;
+    const size_t fixed = part_sorted_smem(P, 0, p2_rows, any_val_null);
+    const size_t per_slot = (size_t)P.slot_bytes + 8;
+    scap2 = budget > fixed + 256 + 2 * per_slot ? (int)((budget - fixed - 256) / per_slot) - 1 : 0;
+    while (scap2 > 0 && part_sorted_smem(P, scap2, p2_rows, any_val_null) > budget) --scap2;
+    scap2 = std::min(scap2, 65000);  // slot indices are 16-bit in the sorted stage
+  } else {
+    scap2 = std::max(0, std::min(220 * 1024, dev.smem_optin - 8192) / P.slot_bytes - 1);
+  }
   const int sfill2 = std::max(1, (int)(scap2 * 0.8));
   bool part_ok = !P.has_arg && !P.need_second_pass && P.num_vals <= 8 && scap2 >= 256;
   for (int v = 0; v < P.num_vals; ++v) part_ok = part_ok && P.vals[v].basic;
@@ -773,7 +794,11 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
         kern<<<grid, nt, psmem, stream>>>(P, A);
       };
       const bool kw1 = P.key_words == 1;
-      switch (opt.scatter) {
+      // 7 (the default): tiles staged by bulk copies when every column allows it
+      std::vector<uint8_t> spec(part_scatter_spec_bytes());
+      const size_t bsm = opt.scatter == 7 ? part_scatter_bulk_plan(P, nparts, dev.smem_optin, spec.data()) : 0;
+      if (bsm) launch_part_scatter_bulk(P, A, spec.data(), bsm, stream);
+      else switch (opt.scatter) {
         case 1: kw1 ? launch(k_part_scatter<1, 16, 256, 3>, 256, 16) : launch(k_part_scatter<2, 16, 256, 3>, 256, 16); break;
         case 2: kw1 ? launch(k_part_scatter<1, 16, 512, 2>, 512, 16) : launch(k_part_scatter<2, 16, 512, 2>, 512, 16); break;
         case 3: kw1 ? launch(k_part_scatter<1, 8, 1024, 1>, 1024, 8) : launch(k_part_scatter<2, 8, 1024, 1>, 1024, 8); break;
@@ -807,8 +832,9 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       for (auto r : prows) nrows += r;
       // a work item is at most a partition's average share, and small
       // enough that few partitions still spread over every SM
+      // (a multiple of 64 rows: pass 2 reads rows in pairs from even starts)
       const int64_t chunk = std::max<int64_t>(
-        32768, std::min<int64_t>(nrows / std::max(1, nparts), nrows / (4 * (int64_t)dev.sms)));
+        32768, std::min<int64_t>(nrows / std::max(1, nparts), nrows / (4 * (int64_t)dev.sms))) & ~(int64_t)63;
       for (int p = 0; p < nparts; ++p) {
         const int64_t r = prows[p];
         if (exact_buckets && r > 2 * chunk) {
@@ -845,8 +871,10 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       ck(cudaMemsetAsync(counters + 6, 0, 8 * 4, stream), "memset");
       G = TableRef{T, spill_cap - 1, P.slot_bytes, P.key_words, counters};
       DenseRef D{dense, dcap, (unsigned long long*)(counters + 10), counters + 6};
-      // shared table plus the all-ones key's slot
-      size_t sm2 = (size_t)(scap2 + 1) * P.slot_bytes;
+      // shared table plus the all-ones key's slot (sorted variants: plus the
+      // count arrays and the chunk's sorted stage)
+      size_t sm2 = p2_sorted ? part_sorted_smem(P, scap2, p2_rows, any_val_null)
+                             : (size_t)(scap2 + 1) * P.slot_bytes;
       // items of split (heavy) partitions first, with rows of one slot
       // combined per warp before their shared update; then the rest
       auto launch2 = [&](auto kern, int nt, int first, int count, unsigned int* work) {
@@ -861,9 +889,21 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
         kern<<<grid, nt, sm2, stream>>>(P2, Ai, G, D, scap2, sfill2, tmpl);
         ++st.kernels;
       };
+      auto launch_s = [&](int first, int count, unsigned int* work, bool wagg) {
+        if (count <= 0) return;
+        PartArgs Ai = A;
+        Ai.items = d_items + first;
+        Ai.nitems = count;
+        Ai.work = work;
+        launch_part_sorted(opt.pass2, P2, Ai, G, D, scap2, sfill2, tmpl, sm2, wagg, stream);
+        ++st.kernels;
+      };
       const bool few = P.num_vals <= 4;
       const int nrest = (int)items.size() - nmerge;
-      if (P.key_words == 1) {
+      if (p2_sorted) {
+        launch_s(0, nmerge, counters + 8, true);
+        launch_s(nmerge, nrest, counters + 9, false);
+      } else if (P.key_words == 1) {
         if (few) {
           launch2(k_part_aggregate<1, 1, 1024, 4, true>, 1024, 0, nmerge, counters + 8);
           launch2(k_part_aggregate<1, 1, 1024, 4, false>, 1024, nmerge, nrest, counters + 9);
@@ -898,6 +938,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
         st.scatter_ms = ms1;
       }
       mark("partition passes (synced)");
+      if (host[14]) throw Error(ERR_CUDA, "partition pass: a bulk copy did not complete in time");
       if (host[5]) break;  // a region overflowed: fall back to the global table
       if (host[1] == 0 && host[6] == 0 && host[13] == 0) {
         done = true;

@@ -77,14 +77,15 @@ struct Options {
   int64_t groups_hint = -1;    // caller's group-count estimate (-1: sample)
   int force_mode = -1;         // -1 auto, 0 global only, 1 smem stage
   int profile = 0;             // time kernels with CUDA events
-  int scatter = 0;             // partitioned pass 1 launch shape (0-6: threads x rows per thread)
+  int scatter = 7;             // partitioned pass 1: 7 bulk-copy tiles where the columns allow, else 0-6 (launch shapes)
+  int pass2 = 0;               // partitioned pass 2: 0 sorted 512x4, 1 per-row reductions, 2 sorted 1024x2, 3 sorted 256x8
   uint32_t set_mask = 0;       // OPT_* bits of the fields a caller set explicitly
 };
 
 // Option fields, as bits of Options::set_mask and TuningRule::mask.
 enum OptBits : uint32_t {
   OPT_BLOCK = 1, OPT_BPS = 2, OPT_SMEM = 4, OPT_FILL = 8, OPT_SMEM_MAX = 16, OPT_LOAD = 32,
-  OPT_MODE = 64, OPT_SCATTER = 128
+  OPT_MODE = 64, OPT_SCATTER = 128, OPT_PASS2 = 256
 };
 
 // A process-wide tuning rule: for calls with at most max_rows rows and at most
@@ -144,5 +145,7 @@ int target_type(int type_id, int kind);
 // with different shared-memory sizes, and a per-launch attribute set by one
 // thread could be lowered by another between its set and its launch.
 void allow_max_smem(const void* kernel);
+// CTAs that fill the device for a kernel at this block size and shared memory
+int grid_for(const void* kernel, int block, size_t smem, int bps_cap);
 
 }  // namespace gb

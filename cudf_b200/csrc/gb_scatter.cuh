@@ -1,0 +1,384 @@
+// gb_scatter.cuh -- pass 1 of the partitioned path with bulk-copy staging.
+//
+// Each CTA takes tiles of T rows.  One thread stages a whole tile into shared
+// memory with cp.async.bulk (global -> shared, completion counted in bytes on
+// an mbarrier): every key column, every value column and every validity mask
+// the plan reads, each as one contiguous copy (the tile's rows of a column are
+// contiguous in HBM).  From the staged tile the threads then
+//   A  pack each row's key, take the top hash bits as partition and the rank
+//      within the tile's partition from a shared histogram;
+//   B  reserve each (tile, partition) run in its region (one global atomic per
+//      partition present) and scan the histogram;
+//   C  write the packed keys at their sorted position, and the inverse
+//      permutation (sorted position -> row) with each position's partition;
+//   D  write every output array of the tile in sorted order: consecutive
+//      threads write consecutive rows of a run, the values gathered from the
+//      staged columns, so no column needs a barrier of its own.
+// Two CTAs share an SM: while one works through a tile, the other's copies are
+// in flight.  Tiles are 16-byte aligned only when every staged column starts
+// on a suitable row (see part_scatter_bulk_ok); the last, partial tile is
+// staged with plain loads.
+//
+// Waits on the mbarrier are bounded: a copy that has not landed after the
+// limit sets counters[14] (the host reports a CUDA error) and the CTA stops
+// after waiting, again bounded, for its copies in flight.
+#pragma once
+#include <cub/block/block_scan.cuh>
+
+#include <cstring>
+
+#include "gb_partition.cuh"
+
+namespace gb {
+
+constexpr int kMaxStaged = 2 * (kMaxKeyCols + 8);
+
+// Arrays a tile stages: data columns (bytes per row = width) and validity
+// masks (one bit per row).  src points at the column's row 0 (offset applied;
+// masks: the word holding row 0, whose bit 0 is row 0).
+struct StageSpec {
+  int32_t narr;
+  int32_t key_data[kMaxKeyCols];  // staged array of key column k
+  int32_t key_mask[kMaxKeyCols];  // its mask array, or -1
+  int32_t val_data[8];
+  int32_t val_mask[8];
+  const uint8_t* src[kMaxStaged];
+  int32_t width[kMaxStaged];      // bytes per row; 0 for a mask
+  int32_t soff[kMaxStaged];       // byte offset in shared memory
+  int32_t stage_bytes;            // all arrays of one tile, with their alignment
+  int32_t tx_bytes;               // bytes the copies of a full tile deliver
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Waits for phase `parity` of the barrier to complete; false after `limit` tries.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int limit)
+{
+  for (int i = 0; i < limit; ++i) {
+    unsigned done;
+    asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// Global -> shared bulk copy of `bytes` (multiple of 16; both addresses
+// 16-byte aligned), counted on `bar`.  The source is this GPU's memory.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                 smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Staged element / validity of a row of the tile.
+__device__ __forceinline__ uint64_t staged_bits(const uint8_t* a, int w, int row)
+{
+  switch (w) {
+    case 1: return a[row];
+    case 2: return ((const uint16_t*)a)[row];
+    case 4: return ((const uint32_t*)a)[row];
+    default: return ((const uint64_t*)a)[row];
+  }
+}
+__device__ __forceinline__ bool staged_valid(const uint8_t* m, int row)
+{
+  return (((const uint32_t*)m)[row >> 5] >> (row & 31)) & 1u;
+}
+
+// Packs the key of staged row `row` (as pack_key does from HBM).
+__device__ __forceinline__ bool pack_key_staged(const Plan& P, const StageSpec& S, const uint8_t* sm, int row,
+                                                uint64_t& w0, uint64_t& w1)
+{
+  w0 = 0;
+  w1 = 0;
+#pragma unroll 1
+  for (int k = 0; k < P.num_keys; ++k) {
+    const KeyCol& c = P.keys[k];
+    if (S.key_mask[k] >= 0 && !staged_valid(sm + S.soff[S.key_mask[k]], row)) {
+      if (!P.include_nulls) return false;
+      const uint64_t nb = 1ull << c.null_shift;
+      if (c.null_word == 0) w0 |= nb;
+      else w1 |= nb;
+      continue;
+    }
+    uint64_t b = staged_bits(sm + S.soff[S.key_data[k]], c.width, row);
+    if (c.cat == CAT_F32) {
+      const float f = __uint_as_float((uint32_t)b);
+      b = f != f ? 0x7FC00000u : (f == 0.0f ? 0 : b);
+    } else if (c.cat == CAT_F64) {
+      const double d = __longlong_as_double((long long)b);
+      b = d != d ? 0x7FF8000000000000ull : (d == 0.0 ? 0 : b);
+    } else if (c.cat == CAT_BOOL) {
+      b = b != 0;
+    }
+    if (c.word == 0) w0 |= b << c.shift;
+    else w1 |= b << c.shift;
+  }
+  return true;
+}
+
+// Shared memory of k_part_scatter_bulk: staged tile | sorted keys (8*KW per
+// row) | order u16[T] | psort u16[T] | hist u32[nparts] | send u32[nparts] |
+// delta i64[nparts]
+inline size_t part_scatter_bulk_smem(const StageSpec& S, int kw, int T, int nparts)
+{
+  auto a16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+  size_t b = a16((size_t)S.stage_bytes);
+  b += a16((size_t)T * 8 * kw);
+  b += a16((size_t)T * 2) * 2;
+  b += a16((size_t)nparts * 4) * 2;
+  b += (size_t)nparts * 8;
+  return b;
+}
+
+template <int KW, int NT, int T>
+__global__ void __launch_bounds__(NT, 2) k_part_scatter_bulk(const __grid_constant__ Plan P,
+                                                             const __grid_constant__ PartArgs A,
+                                                             const __grid_constant__ StageSpec S)
+{
+  static_assert(T % 128 == 0 && T % NT == 0 && T <= 65536, "tile rows");
+  constexpr int RPT = T / NT;
+  extern __shared__ __align__(128) uint8_t sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ unsigned int s_valid, s_stop;
+  using Scan = cub::BlockScan<unsigned, NT>;
+  __shared__ typename Scan::TempStorage scan_tmp;
+  auto a16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+  size_t off = a16((size_t)S.stage_bytes);
+  uint64_t* kst = (uint64_t*)(sm + off);
+  off += a16((size_t)T * 8 * KW);
+  uint16_t* order = (uint16_t*)(sm + off);
+  off += a16((size_t)T * 2);
+  uint16_t* psort = (uint16_t*)(sm + off);
+  off += a16((size_t)T * 2);
+  unsigned int* hist = (unsigned int*)(sm + off);
+  off += a16((size_t)A.nparts * 4);
+  unsigned int* send = (unsigned int*)(sm + off);
+  off += a16((size_t)A.nparts * 4);
+  long long* delta = (long long*)(sm + off);
+  const int64_t n = P.num_rows;
+  const int64_t ntiles = (n + T - 1) / T;
+  const int nv = P.num_vals;
+  const bool any_bits = A.bits != nullptr;
+  const int per = (A.nparts + NT - 1) / NT;
+  constexpr int kWaitLimit = 1 << 22;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_stop = 0;
+  }
+  __syncthreads();
+  // one thread issues a full tile's copies
+  auto issue = [&](int64_t t0) {
+    mbar_expect_tx(&bar, (unsigned)S.tx_bytes);
+#pragma unroll 1
+    for (int a = 0; a < S.narr; ++a) {
+      const int w = S.width[a];
+      const uint8_t* src = w ? S.src[a] + t0 * w : S.src[a] + (t0 >> 3);
+      bulk_g2s(sm + S.soff[a], src, w ? (unsigned)(T * w) : (unsigned)(T / 8), &bar);
+    }
+  };
+  unsigned phase = 0;
+  int64_t tile = blockIdx.x;
+  if (threadIdx.x == 0 && tile < ntiles && (tile + 1) * T <= n) issue(tile * T);
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int64_t t0 = tile * T;
+    const int cnt = (int)min((int64_t)T, n - t0);
+    for (int i = threadIdx.x; i < A.nparts; i += NT) hist[i] = 0;
+    if (cnt == T) {
+      // a full tile: its copies were issued at the end of the previous one
+      const bool ok = mbar_wait(&bar, phase, kWaitLimit);
+      phase ^= 1;
+      if (!ok) {
+        atomicOr(A.counters + 14, 1u);
+        s_stop = 1;
+      }
+    } else {
+      // the partial last tile: plain loads into the same layout
+#pragma unroll 1
+      for (int a = 0; a < S.narr; ++a) {
+        const int w = S.width[a];
+        uint8_t* d = sm + S.soff[a];
+        if (w) {
+          for (int i = threadIdx.x; i < cnt; i += NT) {
+            const uint8_t* s = S.src[a] + (t0 + i) * w;
+            switch (w) {
+              case 1: d[i] = __ldg(s); break;
+              case 2: ((uint16_t*)d)[i] = __ldg((const uint16_t*)s); break;
+              case 4: ((uint32_t*)d)[i] = __ldg((const uint32_t*)s); break;
+              default: ((uint64_t*)d)[i] = __ldg((const unsigned long long*)s); break;
+            }
+          }
+        } else {
+          const uint32_t* s = (const uint32_t*)(S.src[a] + (t0 >> 3));
+          for (int i = threadIdx.x; i < (cnt + 31) / 32; i += NT) ((uint32_t*)d)[i] = __ldg(s + i);
+        }
+      }
+    }
+    __syncthreads();
+    if (s_stop) break;
+    // A: partition and rank of every row (packed keys kept in registers)
+    uint32_t pr[RPT];
+    uint64_t kw0[RPT], kw1[KW == 2 ? RPT : 1];
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+      const int i = k * NT + threadIdx.x;
+      pr[k] = 0xFFFFFFFFu;
+      uint64_t w0 = 0, w1 = 0;
+      if (i < cnt && pack_key_staged(P, S, sm, i, w0, w1)) {
+        const unsigned p = (unsigned)(hash_key(w0, w1, KW) >> A.shift);
+        pr[k] = (p << 16) | atomicAdd(&hist[p], 1u);
+      }
+      kw0[k] = w0;
+      if (KW == 2) kw1[k] = w1;
+    }
+    __syncthreads();
+    // B: reservations, then the scan (as k_part_scatter)
+    unsigned mine = 0;
+    for (int q0 = threadIdx.x * per; q0 < min(A.nparts, (threadIdx.x + 1) * per); q0 += 4) {
+      unsigned h[4];
+      unsigned long long g[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int q = q0 + j;
+        h[j] = (j < per && q < min(A.nparts, (threadIdx.x + 1) * per)) ? hist[q] : 0u;
+        g[j] = h[j] ? atomicAdd(&A.cursor[q], (unsigned long long)h[j]) : 0ull;
+        mine += h[j];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int q = q0 + j;
+        if (!h[j]) continue;
+        const long long room = (long long)A.end[q] - (long long)g[j];
+        if ((long long)h[j] > room) atomicOr(A.counters + 5, 1u);
+        delta[q] = (long long)g[j];
+        send[q] = room <= 0 ? 0u : (unsigned)min((long long)h[j], room);
+      }
+    }
+    unsigned pre, total;
+    Scan(scan_tmp).ExclusiveSum(mine, pre, total);
+    for (int q = threadIdx.x * per; q < min(A.nparts, (threadIdx.x + 1) * per); ++q) {
+      const unsigned h = hist[q];
+      if (h) {
+        delta[q] -= (long long)pre;
+        send[q] += pre;
+      }
+      hist[q] = pre;
+      pre += h;
+    }
+    if (threadIdx.x == 0) s_valid = total;
+    __syncthreads();
+    // C: sorted positions; packed keys at their position
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+      if (pr[k] == 0xFFFFFFFFu) continue;
+      const int i = k * NT + threadIdx.x;
+      const unsigned p = pr[k] >> 16;
+      const unsigned s = hist[p] + (pr[k] & 0xFFFFu);
+      order[s] = (uint16_t)i;
+      psort[s] = (uint16_t)p;
+      kst[KW * s] = kw0[k];
+      if (KW == 2) kst[2 * s + 1] = kw1[k];
+    }
+    __syncthreads();
+    // D: every output array in sorted order
+    const int nvalid = (int)s_valid;
+    for (int s = threadIdx.x; s < nvalid; s += NT) {
+      const unsigned p = psort[s];
+      if ((unsigned)s >= send[p]) continue;
+      const int64_t g = delta[p] + s;
+      const int row = order[s];
+      if (KW == 1) A.keys[g] = kst[s];
+      else *(ulonglong2*)(A.keys + 2 * g) = make_ulonglong2(kst[2 * s], kst[2 * s + 1]);
+      uint32_t vb = 0;
+#pragma unroll 1
+      for (int v = 0; v < nv; ++v) {
+        const int w = P.vals[v].width;
+        const uint64_t x = staged_bits(sm + S.soff[S.val_data[v]], w, row);
+        switch (w) {
+          case 1: ((uint8_t*)A.vals[v])[g] = (uint8_t)x; break;
+          case 2: ((uint16_t*)A.vals[v])[g] = (uint16_t)x; break;
+          case 4: ((uint32_t*)A.vals[v])[g] = (uint32_t)x; break;
+          default: ((uint64_t*)A.vals[v])[g] = x; break;
+        }
+        if (S.val_mask[v] < 0 || staged_valid(sm + S.soff[S.val_mask[v]], row)) vb |= 1u << v;
+      }
+      if (any_bits) A.bits[g] = (uint8_t)vb;
+    }
+    __syncthreads();
+    // the next full tile's copies into the now free stage
+    const int64_t nt = tile + gridDim.x;
+    if (threadIdx.x == 0 && nt < ntiles && (nt + 1) * T <= n) {
+      fence_async_shared();
+      issue(nt * T);
+    }
+  }
+  // leave no copy in flight: a CTA that stopped early waits (bounded) for
+  // the phase it was waiting on
+  if (s_stop && threadIdx.x == 0) mbar_wait(&bar, phase ^ 1, kWaitLimit);
+}
+
+// Whether every array the plan reads can be bulk-copied tile by tile: data
+// 16-byte aligned at row 0 with tile rows a multiple of 16 bytes, masks with
+// row 0 at bit 0 of a 16-byte aligned word; fixed-width types of 1-8 bytes; at
+// most 8 value columns.  Fills S (soff/stage_bytes for tiles of T rows).
+inline bool part_scatter_bulk_ok(const Plan& P, int T, StageSpec& S)
+{
+  std::memset(&S, 0, sizeof(S));
+  if (P.num_vals > 8 || P.num_keys > kMaxKeyCols) return false;
+  int a = 0;
+  size_t off = 0, tx = 0;
+  auto add = [&](const void* data, int64_t offset, int width) -> int {
+    if (a >= kMaxStaged) return -2;
+    const uint8_t* src;
+    if (width) {
+      src = (const uint8_t*)data + offset * width;
+      if (((uintptr_t)src & 15) != 0) return -2;
+    } else {
+      if (offset & 127) return -2;  // row 0 at bit 0 of a 16-byte aligned word
+      src = (const uint8_t*)data + (offset >> 3);
+      if (((uintptr_t)src & 15) != 0) return -2;
+    }
+    S.src[a] = src;
+    S.width[a] = width;
+    S.soff[a] = (int32_t)off;
+    const size_t bytes = width ? (size_t)T * width : (size_t)T / 8;
+    off = (off + bytes + 15) & ~(size_t)15;
+    tx += bytes;
+    return a++;
+  };
+  for (int k = 0; k < P.num_keys; ++k) {
+    const KeyCol& c = P.keys[k];
+    if (c.width != 1 && c.width != 2 && c.width != 4 && c.width != 8) return false;
+    S.key_data[k] = add(c.data, c.offset, c.width);
+    S.key_mask[k] = c.mask ? add(c.mask, c.offset, 0) : -1;
+    if (S.key_data[k] == -2 || S.key_mask[k] == -2) return false;
+  }
+  for (int v = 0; v < P.num_vals; ++v) {
+    const ValCol& c = P.vals[v];
+    if (c.width != 1 && c.width != 2 && c.width != 4 && c.width != 8) return false;
+    S.val_data[v] = add(c.data, c.offset, c.width);
+    S.val_mask[v] = c.mask ? add(c.mask, c.offset, 0) : -1;
+    if (S.val_data[v] == -2 || S.val_mask[v] == -2) return false;
+  }
+  S.narr = a;
+  S.stage_bytes = (int32_t)off;
+  S.tx_bytes = (int32_t)tx;
+  return true;
+}
+
+}  // namespace gb

@@ -88,7 +88,8 @@ typedef struct gb_result {
 } gb_result;
 
 /* Stream-ordered device memory resource (the `mr` of cudf::groupby::aggregate).
- * allocate returns NULL on failure. */
+ * allocate returns NULL on failure, else a block aligned to at least 16 bytes
+ * (RMM's resources give 256). */
 typedef struct gb_allocator {
   void* (*allocate)(void* ctx, size_t bytes, void* stream);
   void (*deallocate)(void* ctx, void* ptr, size_t bytes, void* stream);
@@ -139,9 +140,14 @@ typedef struct gb_tuning {
   int32_t force_mode;
   int64_t groups_hint;      /* caller's estimate of the number of groups (skips sampling) */
   int32_t profile;          /* 1: time the aggregation and compaction kernels with CUDA events */
-  int32_t scatter;          /* partitioned pass 1 launch shape, threads x rows per thread:
-                               0 512x8 (default), 1 256x16, 2 512x16, 3 1024x8, 4 512x8 with the
+  int32_t scatter;          /* partitioned pass 1: 7 (default) tiles of 2048 rows staged in shared
+                               memory by bulk copies when every column allows it (16-byte aligned
+                               rows), else 0; 0-6 the per-thread launch shapes, threads x rows per
+                               thread: 0 512x8, 1 256x16, 2 512x16, 3 1024x8, 4 512x8 with the
                                next column's loads issued early, 5 1024x4, 6 256x8 */
+  int32_t pass2;            /* partitioned pass 2: 0 chunks sorted by slot, 512 threads x 4 rows
+                               (default); 1 per-row shared reductions; 2 as 0; 3 sorted,
+                               256 threads x 8 rows */
 } gb_tuning;
 
 /* What the last gb_aggregate on a handle did. */
@@ -164,7 +170,7 @@ GB_API int gb_set_tuning(gb_handle* handle, const gb_tuning* tuning);
  * rule with rows <= max_rows, groups <= max_groups and a matching key width,
  * and applies the rule's
  * set fields (block, blocks_per_sm, smem_bytes, smem_fill_pct, smem_max_groups,
- * load_factor_pct, force_mode, scatter) except those its handle set with
+ * load_factor_pct, force_mode, scatter, pass2) except those its handle set with
  * gb_set_tuning.  Replaces all rules; NULL/0 clears them.  The rules come
  * from cudf_b200.autotune, which times the candidates per bucket. */
 typedef struct gb_tuning_rule {

@@ -232,6 +232,33 @@ def test_partitioned_mode(nulls, two_word, scatter):
     assert gb.stats()["mode"] == 2
 
 
+@pytest.mark.parametrize("pass2", [0, 1, 3])
+@pytest.mark.parametrize("nulls", [False, True])
+@pytest.mark.parametrize("two_word", [False, True])
+def test_partitioned_pass2_variants(nulls, two_word, pass2):
+    """Pass 2 as chunks sorted by slot (512x4 and 256x8 rows per chunk) and as
+    per-row shared reductions, on every value type of the benchmark."""
+    cb, agg = _cb()
+    rng = np.random.default_rng(39)
+    n = 2_500_000
+    distinct = np.unique(rng.integers(-2**63, 2**63 - 1, 300_000, dtype=np.int64))
+    key = distinct[rng.integers(0, distinct.size, n)]
+    v1 = rng.integers(-10**9, 10**9, n).astype(np.int64)
+    v2 = rng.normal(size=n)
+    v3 = rng.lognormal(size=n).astype(np.float32)
+    v4 = rng.integers(-1000, 1000, n).astype(np.int32)
+    ms = [rng.random(n) > 0.1 if nulls else None for _ in range(4)]
+    keys = [cb.Column.from_numpy(key)]
+    if two_word:
+        keys.append(cb.Column.from_numpy(rng.integers(0, 3, n).astype(np.int16), rng.random(n) > 0.05))
+    aggs = [agg.sum(), agg.count(), agg.min(), agg.max(), agg.mean()]
+    gb, *_ = run_both(keys, [(cb.Column.from_numpy(v1, ms[0]), aggs), (cb.Column.from_numpy(v2, ms[1]), aggs),
+                             (cb.Column.from_numpy(v3, ms[2]), aggs + [agg.count(cb.NullPolicy.INCLUDE)]),
+                             (cb.Column.from_numpy(v4, ms[3]), aggs + [agg.sum_of_squares()])],
+                      include_null_keys=two_word, tuning={"force_mode": 2, "pass2": pass2})
+    assert gb.stats()["mode"] == 2
+
+
 def test_partitioned_mode_is_chosen_for_many_groups():
     cb, agg = _cb()
     rng = np.random.default_rng(32)
@@ -242,8 +269,9 @@ def test_partitioned_mode_is_chosen_for_many_groups():
     assert gb.stats()["mode"] == 2
 
 
+@pytest.mark.parametrize("pass2", [0, 1, 3])
 @pytest.mark.parametrize("scatter", [0, 1])
-def test_partitioned_spill_when_groups_underestimated(scatter):
+def test_partitioned_spill_when_groups_underestimated(scatter, pass2):
     cb, agg = _cb()
     rng = np.random.default_rng(33)
     n = 1_500_000
@@ -253,11 +281,12 @@ def test_partitioned_spill_when_groups_underestimated(scatter):
     f = rng.random(n).astype(np.float32)
     run_both([cb.Column.from_numpy(key)], [(cb.Column.from_numpy(v), [agg.sum(), agg.count(), agg.min()]),
                                            (cb.Column.from_numpy(f, rng.random(n) > 0.2), [agg.mean(), agg.max()])],
-             tuning={"force_mode": 2, "groups_hint": 1000, "scatter": scatter})
+             tuning={"force_mode": 2, "groups_hint": 1000, "scatter": scatter, "pass2": pass2})
 
 
+@pytest.mark.parametrize("pass2", [0, 1, 3])
 @pytest.mark.parametrize("scatter", [0, 1])
-def test_partitioned_all_ones_key_heavy(scatter):
+def test_partitioned_all_ones_key_heavy(scatter, pass2):
     """40% of the rows carry the all-ones key: one partition aggregates them in
     its dedicated shared slot, merged into the global table's slot at flush."""
     cb, agg = _cb()
@@ -270,11 +299,12 @@ def test_partitioned_all_ones_key_heavy(scatter):
     gb, *_ = run_both([cb.Column.from_numpy(key)],
                       [(cb.Column.from_numpy(v, rng.random(n) > 0.1), [agg.sum(), agg.count(), agg.min(), agg.max()]),
                        (cb.Column.from_numpy(d, rng.random(n) > 0.1), [agg.mean(), agg.min(), agg.max()])],
-                      tuning={"force_mode": 2, "scatter": scatter})
+                      tuning={"force_mode": 2, "scatter": scatter, "pass2": pass2})
     assert gb.stats()["mode"] == 2
 
 
-def test_partitioned_skew_splits_heavy_partitions():
+@pytest.mark.parametrize("pass2", [0, 1, 3])
+def test_partitioned_skew_splits_heavy_partitions(pass2):
     """Zipf(1.3) keys: a few keys hold a large share of the rows; their
     partitions are cut into row ranges whose tables merge globally."""
     cb, agg = _cb()
@@ -283,12 +313,13 @@ def test_partitioned_skew_splits_heavy_partitions():
     key = (rng.zipf(1.3, n) % 1_000_003).astype(np.int64)
     v = rng.integers(0, 1000, n).astype(np.int64)
     gb, *_ = run_both([cb.Column.from_numpy(key)], [(cb.Column.from_numpy(v), [agg.sum(), agg.count(), agg.max()])],
-                      tuning={"force_mode": 2})
+                      tuning={"force_mode": 2, "pass2": pass2})
     assert gb.stats()["mode"] == 2
 
 
+@pytest.mark.parametrize("pass2", [0, 1, 3])
 @pytest.mark.parametrize("hot_frac", [0.5, 0.95])
-def test_partitioned_hot_key_warp_combined_updates(hot_frac):
+def test_partitioned_hot_key_warp_combined_updates(hot_frac, pass2):
     """One key holds most rows: its partition is split and each warp combines
     the hot key's values before one shared update, for every value type and
     accumulator the partitioned path takes."""
@@ -311,14 +342,15 @@ def test_partitioned_hot_key_warp_combined_updates(hot_frac):
     reqs = []
     for (v, m), t in zip(cols, types):
         reqs.append((cb.Column.from_numpy(v, m, t) if t is not None else cb.Column.from_numpy(v, m), aggs))
-    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs[:4], tuning={"force_mode": 2})
+    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs[:4], tuning={"force_mode": 2, "pass2": pass2})
     assert gb.stats()["mode"] == 2
-    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs[4:], tuning={"force_mode": 2})
+    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs[4:], tuning={"force_mode": 2, "pass2": pass2})
     assert gb.stats()["mode"] == 2
 
 
+@pytest.mark.parametrize("pass2", [0, 1])
 @pytest.mark.parametrize("include", [False, True])
-def test_zipf_pairs_two_word_keys(include):
+def test_zipf_pairs_two_word_keys(include, pass2):
     """The shape of the high-cardinality benchmark at 4M rows: (int32, int64)
     keys = divmod(p, 1000) with p Zipf-skewed, 5% nulls per key column."""
     cb, agg = _cb()
@@ -333,7 +365,7 @@ def test_zipf_pairs_two_word_keys(include):
     vf = rng.random(n)
     aggs = [agg.sum(), agg.count(), agg.max()]
     gb, *_ = run_both([k1, k2], [(cb.Column.from_numpy(vi), aggs), (cb.Column.from_numpy(vf), aggs)],
-                      include_null_keys=include)
+                      include_null_keys=include, tuning={"pass2": pass2})
     assert gb.stats()["mode"] == 2
 
 
@@ -467,7 +499,8 @@ def test_shared_stage_row_ranges_match_both_kernels(policy):
     assert gb.stats()["mode"] == 1
 
 
-def test_partitioned_many_partitions_wide_slots():
+@pytest.mark.parametrize("pass2", [0, 1])
+def test_partitioned_many_partitions_wide_slots(pass2):
     """Wide slots (eight value columns) leave ~1000 slots per shared table, so
     3.5M groups need 8192 partitions; every group and value must still match."""
     cb, agg = _cb()
@@ -479,5 +512,5 @@ def test_partitioned_many_partitions_wide_slots():
         v = rng.integers(-10**9, 10**9, n).astype(np.int64)
         reqs.append((cb.Column.from_numpy(v, rng.random(n) > 0.1 if i % 2 else None),
                      [agg.sum(), agg.min(), agg.max()]))
-    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs)
+    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs, tuning={"pass2": pass2})
     assert gb.stats()["mode"] == 2
