@@ -69,7 +69,8 @@ class GbBatchStats(ctypes.Structure):
 class GbServerOptions(ctypes.Structure):
     _fields_ = [("memory_cap_bytes", ctypes.c_int64), ("max_batch_queries", ctypes.c_int32),
                 ("max_batch_rows", ctypes.c_int64), ("workers", ctypes.c_int32),
-                ("direct_rows", ctypes.c_int64), ("direct_groups", ctypes.c_int64)]
+                ("direct_rows", ctypes.c_int64), ("direct_groups", ctypes.c_int64),
+                ("reserve_bytes", ctypes.c_int64)]
 
 
 class GbQueryInfo(ctypes.Structure):
@@ -82,7 +83,8 @@ class GbServerStats(ctypes.Structure):
                 ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double), ("queries_per_s", ctypes.c_double),
                 ("peak_admitted_bytes", ctypes.c_int64), ("sketch_s", ctypes.c_double),
                 ("prepare_s", ctypes.c_double), ("run_s", ctypes.c_double), ("trial_rounds", ctypes.c_int64),
-                ("direct_runs", ctypes.c_int64)]
+                ("direct_runs", ctypes.c_int64), ("held_for_memory", ctypes.c_int64),
+                ("min_free_bytes", ctypes.c_int64)]
 
 
 class GroupbyError(RuntimeError):

@@ -756,7 +756,11 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   TableRef G{};
   uint8_t* dense = nullptr;
   int64_t dense_n = 0;
+  int64_t dense_cap = 0;
   bool done = false;
+  // one read-back for the whole call (see Options::sync_checks)
+  const bool deferred = !opt.sync_checks;
+  bool prof_part = false, prof_agg = false;
 
   if (mode == 2) {
     // ---- pass 1: scatter rows into hash partitions ----
@@ -860,6 +864,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     uint32_t spill_list = (uint32_t)std::min<uint64_t>(
       1ull << 31, next_pow2((uint64_t)std::max<double>(262144.0, 4.0 * expect_spill)));
     int64_t dcap = (int64_t)(est * 1.5) + (int64_t)nparts * 256 + 4096;
+    dense_cap = dcap;
     for (int attempt = 0;; ++attempt) {
       T = (uint8_t*)S.get((size_t)(spill_cap + 1) * P.slot_bytes);
       dense = (uint8_t*)S.get((size_t)dcap * P.slot_bytes);
@@ -928,6 +933,14 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       k_finish_count<<<1, 1, 0, stream>>>(P, G);
       st.kernels += 3;
       ck(cudaGetLastError(), "partition aggregate launch");
+      if (deferred) {
+        // counts and flags stay on the device until the compaction is done
+        done = true;
+        dense_n = -1;
+        cap = spill_cap;
+        prof_part = opt.profile;
+        break;
+      }
       ck(cudaMemcpyAsync(host, counters, 64, cudaMemcpyDeviceToHost, stream), "d2h");
       ck(cudaStreamSynchronize(stream), "partition sync");
       if (opt.profile && attempt == 0) {
@@ -1038,6 +1051,10 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       k_finish_count<<<1, 1, 0, stream>>>(P, G);
       st.kernels += 3;
       ck(cudaGetLastError(), "aggregate launch");
+      if (deferred) {
+        prof_agg = opt.profile;
+        break;
+      }
       ck(cudaMemcpyAsync(host, counters, 64, cudaMemcpyDeviceToHost, stream), "count d2h");
       ck(cudaStreamSynchronize(stream), "aggregate sync");
       if (raw_stage && host[13]) {
@@ -1060,7 +1077,9 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   }
   st.capacity = (int64_t)cap;
   mark("aggregate done");
-  const int64_t G_n = (int64_t)host[0] + dense_n;
+  // deferred: outputs are sized for every slot that could hold a group
+  int64_t G_n = deferred ? -1 : (int64_t)host[0] + dense_n;
+  const int64_t out_rows = deferred ? (dense ? dense_cap : 0) + (int64_t)cap + 1 : G_n;
   R.num_groups = G_n;
 
   if (P.need_second_pass) {
@@ -1075,7 +1094,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     OutPtrs O;
     std::memset(&O, 0, sizeof(O));
     for (int k = 0; k < P.num_keys; ++k) {
-      R.keys.push_back(make_out(alloc, stream, keys[k].type_id, G_n, keys[k].mask != nullptr));
+      R.keys.push_back(make_out(alloc, stream, keys[k].type_id, out_rows, keys[k].mask != nullptr));
       O.key_data[k] = R.keys.back().data;
       O.key_mask[k] = R.keys.back().mask;
     }
@@ -1084,43 +1103,86 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       for (auto& r : reqs) {
         std::vector<OutColumn> cols;
         for (size_t a = 0; a < r.aggs.size(); ++a, ++j) {
-          cols.push_back(make_out(alloc, stream, out_types[j], G_n, P.outs[j].nullable));
+          cols.push_back(make_out(alloc, stream, out_types[j], out_rows, P.outs[j].nullable));
           O.out_data[j] = cols.back().data;
           O.out_mask[j] = cols.back().mask;
         }
         R.results.push_back(cols);
       }
     }
-    O.counters = counters;
-    ck(cudaMemsetAsync(counters, 0, 512, stream), "memset");  // position + null counters
+    // position and null counters of the compaction, apart from the
+    // aggregation's counts and flags in counters[0, 16)
+    unsigned int* ccount = counters + 256;
+    uint32_t* chost = host + 256;
+    O.counters = ccount;
+    ck(cudaMemsetAsync(ccount, 0, 512, stream), "memset");
     if (opt.profile) ck(cudaEventRecord(events()[2], stream), "event");
-    if (dense_n > 0) {
+    const int64_t limit = deferred ? out_rows : G_n;
+    if (deferred && dense) {
+      int grid = (int)std::min<int64_t>((dense_cap + 255) / 256, (int64_t)dev.sms * 8);
+      k_compact<<<grid, 256, 0, stream>>>(P, dense, dense_cap, P.slot_bytes, limit, 1, O,
+                                          (const unsigned long long*)(counters + 10));
+      ++st.kernels;
+    } else if (dense_n > 0) {
       int grid = (int)std::min<int64_t>((dense_n + 255) / 256, (int64_t)dev.sms * 8);
-      k_compact<<<grid, 256, 0, stream>>>(P, dense, dense_n, P.slot_bytes, G_n, 1, O);
+      k_compact<<<grid, 256, 0, stream>>>(P, dense, dense_n, P.slot_bytes, limit, 1, O);
       ++st.kernels;
     }
-    if (G_n > dense_n) {
+    if (deferred || G_n > dense_n) {
       int64_t nslots = (int64_t)cap + 1;
       int grid = (int)std::min<int64_t>((nslots + 255) / 256, (int64_t)dev.sms * 8);
-      k_compact<<<grid, 256, 0, stream>>>(P, T, nslots, P.slot_bytes, G_n, 0, O);
+      k_compact<<<grid, 256, 0, stream>>>(P, T, nslots, P.slot_bytes, limit, 0, O);
       ++st.kernels;
     }
     if (opt.profile) ck(cudaEventRecord(events()[3], stream), "event");
     ck(cudaGetLastError(), "compact launch");
-    ck(cudaMemcpyAsync(host, counters, 4 * (4 + P.num_keys + P.num_outs), cudaMemcpyDeviceToHost, stream),
+    if (deferred) ck(cudaMemcpyAsync(host, counters, 64, cudaMemcpyDeviceToHost, stream), "counts d2h");
+    ck(cudaMemcpyAsync(chost, ccount, 4 * (4 + P.num_keys + P.num_outs), cudaMemcpyDeviceToHost, stream),
        "null counts d2h");
     ck(cudaStreamSynchronize(stream), "compact sync");
-    if (host[1]) throw Error(ERR_CUDA, "internal error: compaction found more groups than were counted");
     mark("compaction (synced)");
+    if (deferred) {
+      if (host[14]) throw Error(ERR_CUDA, "partition pass: a bulk copy did not complete in time");
+      // an overflow anywhere (a table, a region, the dense slots, a spill
+      // list): redo the call with checks after every stage
+      const bool again = host[1] || chost[1] || (mode == 2 && (host[5] || host[6] || host[13])) ||
+                         (raw_stage && host[13]);
+      if (again) {
+        R.release();
+        Options o2 = opt_in;
+        o2.sync_checks = 1;
+        return aggregate(keys, null_policy, reqs, stream, alloc, o2, stats);
+      }
+      const int64_t dn = mode == 2 ? (int64_t)(host[10] | ((uint64_t)host[11] << 32)) : 0;
+      G_n = (int64_t)chost[2];
+      if (G_n != (int64_t)host[0] + dn)
+        throw Error(ERR_CUDA, "internal error: compaction wrote " + std::to_string(G_n) + " groups of " +
+                                  std::to_string((int64_t)host[0] + dn));
+      R.num_groups = G_n;
+      for (auto& c : R.keys) c.size = G_n;
+      for (auto& cols : R.results)
+        for (auto& c : cols) c.size = G_n;
+      if (prof_part || prof_agg) {
+        float ms = 0, ms1 = 0;
+        ck(cudaEventElapsedTime(&ms, events()[0], events()[1]), "event time");
+        st.agg_kernel_ms += ms;
+        if (prof_part) {
+          ck(cudaEventElapsedTime(&ms1, events()[0], events()[4]), "event time");
+          st.scatter_ms = ms1;
+        }
+      }
+    } else if (chost[1]) {
+      throw Error(ERR_CUDA, "internal error: compaction found more groups than were counted");
+    }
     if (opt.profile) {
       float ms = 0;
       ck(cudaEventElapsedTime(&ms, events()[2], events()[3]), "event time");
       st.compact_ms = ms;
     }
-    for (int k = 0; k < P.num_keys; ++k) R.keys[k].null_count = host[4 + k];
+    for (int k = 0; k < P.num_keys; ++k) R.keys[k].null_count = chost[4 + k];
     int j = 0;
     for (auto& cols : R.results)
-      for (auto& c : cols) c.null_count = host[4 + P.num_keys + j++];
+      for (auto& c : cols) c.null_count = chost[4 + P.num_keys + j++];
   } catch (...) {
     R.release();
     throw;

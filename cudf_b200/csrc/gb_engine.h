@@ -80,6 +80,11 @@ struct Options {
   int scatter = 7;             // partitioned pass 1: 7 bulk-copy tiles where the columns allow, else 0-6 (launch shapes)
   int pass2 = 0;               // partitioned pass 2: 0 sorted 512x4, 1 per-row reductions, 2 sorted 1024x2, 3 sorted 256x8
   uint32_t set_mask = 0;       // OPT_* bits of the fields a caller set explicitly
+  // internal: 0 reads every outcome (group counts, overflow flags, null
+  // counts) back once, after the compaction, sizing the outputs by an upper
+  // bound; a call whose flags show an overflow is redone with 1, which checks
+  // after each stage and regrows tables as it goes
+  int sync_checks = 0;
 };
 
 // Option fields, as bits of Options::set_mask and TuningRule::mask.

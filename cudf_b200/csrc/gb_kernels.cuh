@@ -383,13 +383,17 @@ __device__ __forceinline__ void compact_block(const Plan& P, const uint8_t* T, i
   __syncthreads();
 }
 
+// nslots_dev (optional): a device count that bounds nslots (dense slots
+// written by the partitioned pass, read here instead of on the host).
 static __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ Plan P, const uint8_t* T,
                                                         int64_t nslots, int stride, int64_t limit, int dense,
-                                                        const __grid_constant__ OutPtrs O)
+                                                        const __grid_constant__ OutPtrs O,
+                                                        const unsigned long long* nslots_dev = nullptr)
 {
   using Scan = cub::BlockScan<int, 256>;
   __shared__ typename Scan::TempStorage tmp;
   __shared__ unsigned int s_base;
+  if (nslots_dev) nslots = min(nslots, (int64_t)*(volatile const unsigned long long*)nslots_dev);
   const int64_t step = (int64_t)gridDim.x * blockDim.x;
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < nslots; base += step)
     compact_block(P, T, nslots, stride, limit, dense, O, base, &tmp, &s_base);

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <condition_variable>
 #include <cstring>
@@ -83,6 +84,7 @@ struct Server {
   double first_arrive = -1, last_done = 0;
   double sketch_s = 0, prepare_s = 0, run_s = 0, trial_s = 0;
   int64_t trial_rounds = 0, direct_runs = 0;
+  int64_t held_for_memory = 0, min_free = -1;
   cudaStream_t sketch_stream = nullptr;
 
   // device-side sketch of a set of queries: estimated groups per query, one
@@ -156,8 +158,22 @@ struct Server {
           waiting.push_back(arrivals[i]);
         }
       }
-      // admission in arrival order under the memory cap; pack into batches
+      // admission in arrival order under the memory cap and the device's free
+      // memory (less a reserve); pack into batches.  Free memory already
+      // counts what running queries allocated; this round's admissions are
+      // charged against it as they are admitted.
       std::vector<std::shared_ptr<Query>> admitted;
+      int64_t free_budget = INT64_MAX;
+      if (!waiting.empty()) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+          free_budget = (int64_t)fr - opt.reserve_bytes;
+          std::lock_guard<std::mutex> lk(mu);
+          min_free = min_free < 0 ? (int64_t)fr : std::min(min_free, (int64_t)fr);
+        } else {
+          cudaGetLastError();
+        }
+      }
       {
         std::unique_lock<std::mutex> lk(mu);
         int64_t rows = 0;
@@ -172,6 +188,11 @@ struct Server {
             continue;
           }
           if (in_use + q->est_bytes > opt.memory_cap_bytes && in_use > 0) break;
+          if (q->est_bytes > free_budget && in_use > 0) {
+            ++held_for_memory;
+            break;
+          }
+          free_budget -= q->est_bytes;
           if ((int)admitted.size() >= opt.max_batch_queries) break;
           in_use += q->est_bytes;
           peak_in_use = std::max(peak_in_use, in_use);
@@ -387,6 +408,7 @@ int gb_server_create(const gb_server_options* opt, gb_server** out)
     S.opt.workers = 4;
     S.opt.direct_rows = 64 << 10;
     S.opt.direct_groups = 64 << 10;
+    S.opt.reserve_bytes = 2ll << 30;
     if (opt) {
       if (opt->memory_cap_bytes > 0) S.opt.memory_cap_bytes = opt->memory_cap_bytes;
       if (opt->max_batch_queries > 0) S.opt.max_batch_queries = opt->max_batch_queries;
@@ -394,6 +416,7 @@ int gb_server_create(const gb_server_options* opt, gb_server** out)
       if (opt->workers > 0) S.opt.workers = std::min(8, opt->workers);
       if (opt->direct_rows > 0) S.opt.direct_rows = opt->direct_rows;
       if (opt->direct_groups > 0) S.opt.direct_groups = opt->direct_groups;
+      if (opt->reserve_bytes > 0) S.opt.reserve_bytes = opt->reserve_bytes;
     }
     if (cudaGetDevice(&S.device) != cudaSuccess) throw gb::Error(gb::ERR_CUDA, "cudaGetDevice failed");
     S.threads.emplace_back([&S] { S.dispatcher(); });
@@ -533,6 +556,8 @@ int gb_server_get_stats(gb_server* sv, gb_server_stats* out)
     out->run_s = S.run_s;
     out->trial_rounds = S.trial_rounds;
     out->direct_runs = S.direct_runs;
+    out->held_for_memory = S.held_for_memory;
+    out->min_free_bytes = S.min_free;
   });
 }
 

@@ -38,10 +38,10 @@ def _close_open_servers():
 class Server:
     def __init__(self, memory_cap_bytes: int = 150 << 30, max_batch_queries: int = 256,
                  max_batch_rows: int = 400 << 20, workers: int = 4, direct_rows: int = 0,
-                 direct_groups: int = 0):
+                 direct_groups: int = 0, reserve_bytes: int = 0):
         L = _lib.lib()
         o = _lib.GbServerOptions(memory_cap_bytes, max_batch_queries, max_batch_rows, workers,
-                                 direct_rows, direct_groups)
+                                 direct_rows, direct_groups, reserve_bytes)
         h = ctypes.c_void_p()
         _lib.check(L.gb_server_create(ctypes.byref(o), ctypes.byref(h)))
         self._h = h

@@ -262,6 +262,8 @@ typedef struct gb_server_options {
   int64_t direct_rows;        /* queries with at least this many rows run alone through the
                                  single-query engine (default 64 Ki) ... */
   int64_t direct_groups;      /* ... as do queries with more estimated groups (default 64 Ki) */
+  int64_t reserve_bytes;      /* device memory admission leaves free (cudaMemGetInfo), beside the
+                                 cap (default 2 GiB) */
 } gb_server_options;
 typedef struct gb_query_info {
   int32_t status;             /* 2 done, 3 failed */
@@ -282,6 +284,8 @@ typedef struct gb_server_stats {
   double run_s;               /* workers' batch run time */
   int64_t trial_rounds;
   int64_t direct_runs;        /* large, many-group queries run alone instead of batched */
+  int64_t held_for_memory;    /* admission rounds that stopped at free device memory */
+  int64_t min_free_bytes;     /* lowest free device memory seen at admission */
 } gb_server_stats;
 GB_API int gb_server_create(const gb_server_options* opt, gb_server** out);
 GB_API int gb_server_submit(gb_server* server, const gb_column* keys, int32_t num_keys, int32_t null_policy,

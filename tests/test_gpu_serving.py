@@ -131,3 +131,26 @@ def test_large_queries_run_alone_and_match():
         srv.release(ids[i])
     assert srv.stats()["direct_runs"] >= 1
     srv.close()
+
+
+def test_admission_by_free_device_memory_holds_then_completes():
+    """A reserve that leaves less free device memory than one query needs:
+    admission waits on free memory (one query at a time runs), yet every
+    query completes with the oracle's result."""
+    cb, _ = _cb()
+    qs = _queries(44, 6)
+    dev = [_dev(q) for q in qs]
+    torch.cuda.synchronize()
+    free, _ = torch.cuda.mem_get_info()
+    srv = cb.Server(workers=2, reserve_bytes=free)  # nothing is left above the reserve
+    ids = [srv.submit(*d) for d in dev]
+    for i, q in enumerate(qs):
+        assert srv.wait(ids[i], timeout_s=120)["status"] == 2
+        uk, res = srv.result(ids[i])
+        _check(q, uk, res)
+        srv.release(ids[i])
+    st = srv.stats()
+    assert st["completed"] == len(qs) and st["failed"] == 0
+    # a query waits while an earlier one is admitted and unreleased
+    assert st["held_for_memory"] >= 1 and 0 < st["min_free_bytes"] <= free
+    srv.close()
