@@ -63,7 +63,17 @@ class GbTuningRule(ctypes.Structure):
 class GbBatchStats(ctypes.Structure):
     _fields_ = [("instances", ctypes.c_int64), ("tiles", ctypes.c_int64), ("smem_instances", ctypes.c_int64),
                 ("table_bytes", ctypes.c_int64), ("output_bytes", ctypes.c_int64),
-                ("kernels_per_run", ctypes.c_int32), ("regrown", ctypes.c_int64)]
+                ("kernels_per_run", ctypes.c_int32), ("regrown", ctypes.c_int64), ("block", ctypes.c_int32),
+                ("tile_rows", ctypes.c_int64), ("ruled_instances", ctypes.c_int64)]
+
+
+class GbBatchRule(ctypes.Structure):
+    _fields_ = [("max_rows", ctypes.c_int64), ("max_groups", ctypes.c_int64), ("smem_slots", ctypes.c_int32),
+                ("headroom_pct", ctypes.c_int32)]
+
+
+class GbBatchLaunch(ctypes.Structure):
+    _fields_ = [("block", ctypes.c_int32), ("tile_rows", ctypes.c_int32), ("smem_bytes", ctypes.c_int32)]
 
 
 class GbServerOptions(ctypes.Structure):
@@ -129,6 +139,8 @@ SIGNATURES = {
                                        ctypes.POINTER(GbOutColumn), ctypes.POINTER(GbOutColumn)]),
     "gb_batch_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GbBatchStats)]),
     "gb_batch_destroy": (None, [ctypes.c_void_p]),
+    "gb_batch_set_tuning": (ctypes.c_int, [ctypes.POINTER(GbBatchRule), ctypes.c_int32,
+                                           ctypes.POINTER(GbBatchLaunch)]),
     "gb_server_create": (ctypes.c_int, [ctypes.POINTER(GbServerOptions), ctypes.POINTER(ctypes.c_void_p)]),
     "gb_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GbColumn), ctypes.c_int32, ctypes.c_int32,
                                         ctypes.POINTER(GbRequest), ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]),

@@ -11,6 +11,12 @@ sketch has estimated the groups.
 
     python -m cudf_b200.autotune --out cudf_b200/tuning_b200.json   # on a B200
 
+Batched launches (``gb_batch_set_tuning``) are tuned the same way: the
+aggregation kernel's block size, rows per tile and shared-table budget on a
+mix drawn like the batched benchmark, then per instance size bucket the
+shared-stage rule (table headroom, or the global table only) that runs a batch
+of that bucket fastest.
+
 ``cudf_b200`` installs ``tuning_b200.json`` (next to this file) at import
 when it exists; ``load(path)`` / ``clear()`` change that at run time.
 """
@@ -74,9 +80,133 @@ def save(rules: Sequence[Dict], path: str, meta: Optional[Dict] = None) -> None:
 
 def load(path: str = TUNING_FILE) -> List[Dict]:
     with open(path) as f:
-        rules = json.load(f)["rules"]
+        d = json.load(f)
+    rules = d["rules"]
     set_rules(rules)
+    if "batch" in d:
+        set_batch_tuning(d["batch"].get("rules", []), d["batch"].get("launch"))
     return rules
+
+
+# -- batched launches (gb_batch_set_tuning) -------------------------------------
+def set_batch_tuning(rules: Sequence[Dict], launch: Optional[Dict] = None) -> None:
+    """Installs batch tuning: launch {"block", "tile_rows", "smem_bytes"} and
+    per-instance rules [{"max_rows", "max_groups", "smem_slots", "headroom_pct"}]
+    (first match applies; -1 / 0 leave a field unset)."""
+    arr = (_lib.GbBatchRule * max(1, len(rules)))()
+    for i, r in enumerate(rules):
+        arr[i] = _lib.GbBatchRule(int(r["max_rows"]), int(r["max_groups"]), int(r.get("smem_slots", -1)),
+                                  int(r.get("headroom_pct", 0)))
+    lp = None
+    if launch:
+        lp = ctypes.byref(_lib.GbBatchLaunch(int(launch["block"]), int(launch["tile_rows"]),
+                                             int(launch["smem_bytes"])))
+    _lib.check(_lib.lib().gb_batch_set_tuning(arr, len(rules), lp))
+
+
+BATCH_LAUNCH_DEFAULT = {"block": 512, "tile_rows": 65536, "smem_bytes": 160 * 1024}
+_BATCH_BLOCKS = [256, 512, 1024]
+_BATCH_TILES = [16384, 65536, 262144]
+_BATCH_SMEM = [96 * 1024, 160 * 1024, 200 * 1024]
+# instance buckets (rows x estimated groups) of the per-instance rules
+BATCH_BUCKETS = [(r, g) for r in (16384, 262144, 4194304) for g in (256, 4096, 65536, 1 << 30)]
+_BATCH_RULE_CANDS = [{"headroom_pct": 150}, {"headroom_pct": 200}, {"headroom_pct": 400}, {"smem_slots": 0}]
+
+
+def _batch_workload(sizes, seed: int):
+    """Instances with the batched benchmark's schema: int32 keys uniform over
+    each instance's cardinality, int64 [0, 1e6] and float64 normal values with
+    5% nulls, sum/count/min/max/mean.  sizes: [(rows, cardinality)]."""
+    import torch
+    from . import aggregation as agg
+    from .column import Column, Table, pack_mask
+    from .groupby import GroupByRequest
+    from .types import TypeId
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    inst = []
+    for n, c in sizes:
+        k = torch.randint(0, max(1, int(c)), (int(n),), device="cuda", generator=g, dtype=torch.int32)
+        v1 = torch.randint(0, 10**6 + 1, (int(n),), device="cuda", generator=g, dtype=torch.int64)
+        v2 = torch.randn(int(n), device="cuda", generator=g, dtype=torch.float64)
+        m1 = pack_mask(torch.rand(int(n), device="cuda", generator=g) >= 0.05)
+        m2 = pack_mask(torch.rand(int(n), device="cuda", generator=g) >= 0.05)
+        aggs = [agg.sum(), agg.count(), agg.min(), agg.max(), agg.mean()]
+        inst.append((Table([Column(TypeId.INT32, k)]),
+                     [GroupByRequest(Column(TypeId.INT64, v1, m1), aggs),
+                      GroupByRequest(Column(TypeId.FLOAT64, v2, m2), aggs)]))
+    return inst
+
+
+def _time_batch(inst, steps: int) -> float:
+    import torch
+    from .batch import BatchGroupBy
+    bg = BatchGroupBy(inst, use_graph=True)
+    bg.run()
+    stream = torch.cuda.current_stream()
+    times = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        bg.run()
+        b.record(stream)
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    times.sort()
+    return times[len(times) // 2]
+
+
+def tune_batch(instances: int = 512, steps: int = 3, verbose: bool = False) -> Tuple[Dict, Dict]:
+    """Launch settings on a mix drawn like the batched benchmark (rows
+    log-uniform [1e3, 4e6], cardinality log-uniform [4, 1e5]) by coordinate
+    descent over block, tile rows and table budget; then, per instance size
+    bucket, the shared-stage rule that runs a batch of that bucket fastest."""
+    import numpy as np
+    rng = np.random.default_rng(11)
+    rows = np.exp(rng.uniform(np.log(1e3), np.log(4e6), instances)).astype(np.int64)
+    cards = np.exp(rng.uniform(np.log(4), np.log(1e5), instances)).astype(np.int64)
+    mix = _batch_workload(list(zip(rows.tolist(), cards.tolist())), 12)
+    log: Dict[str, object] = {}
+    set_batch_tuning([], BATCH_LAUNCH_DEFAULT)
+    best = dict(BATCH_LAUNCH_DEFAULT)
+    best_ms = _time_batch(mix, steps)
+    log["launch default"] = best_ms
+    for field, cands in (("block", _BATCH_BLOCKS), ("tile_rows", _BATCH_TILES), ("smem_bytes", _BATCH_SMEM)):
+        for v in cands:
+            t = dict(best)
+            t[field] = v
+            set_batch_tuning([], t)
+            ms = _time_batch(mix, steps)
+            log["launch " + json.dumps(t)] = ms
+            if ms < best_ms * 0.98:
+                best, best_ms = t, ms
+    del mix
+    rules = []
+    for r_hi, g_hi in BATCH_BUCKETS:
+        lo_r = 4097 if r_hi == 16384 else r_hi // 16
+        sizes = []
+        for _ in range(32 if r_hi <= 262144 else 8):
+            n = int(np.exp(rng.uniform(np.log(lo_r), np.log(r_hi))))
+            g = int(min(n, np.exp(rng.uniform(np.log(max(2, g_hi // 16)), np.log(min(g_hi, 1 << 20))))))
+            sizes.append((n, max(2, g)))
+        inst = _batch_workload(sizes, r_hi ^ g_hi)
+        cand_best, cand_ms = None, None
+        for cand in [{}] + _BATCH_RULE_CANDS:
+            rule = {"max_rows": r_hi, "max_groups": g_hi, **cand}
+            set_batch_tuning([rule] if cand else [], best)
+            ms = _time_batch(inst, steps)
+            log[f"bucket {r_hi}x{g_hi} {json.dumps(cand)}"] = ms
+            if cand_ms is None or ms < cand_ms * 0.98:
+                cand_best, cand_ms = cand, ms
+        if cand_best:
+            rules.append({"max_rows": r_hi, "max_groups": g_hi, **cand_best})
+        if verbose:
+            print(f"batch bucket rows<={r_hi} groups<={g_hi}: {cand_best} {cand_ms:.3f} ms", flush=True)
+        del inst
+    set_batch_tuning(rules, best)
+    if verbose:
+        print(f"batch launch: {best} {best_ms:.3f} ms", flush=True)
+    return {"launch": best, "rules": rules}, {"launch_ms": best_ms, "trials": log}
 
 
 def order_rules(rules: Sequence[Dict]) -> List[Dict]:
@@ -173,14 +303,28 @@ def main():
     ap.add_argument("--out", default=TUNING_FILE)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--max-rows", type=int, default=1 << 27, help="skip buckets with more rows")
+    ap.add_argument("--what", default="all", choices=["all", "single", "batch"],
+                    help="tune single-query rules, batched launches, or both (the other part of an "
+                         "existing file is kept)")
     args = ap.parse_args()
     import torch
     name = torch.cuda.get_device_name(0)
-    buckets = [b for b in DEFAULT_BUCKETS if b[0] <= args.max_rows]
-    rules, meta = tune(buckets, args.steps, verbose=True)
-    meta["device"] = name
-    save(rules, args.out, meta)
-    print(f"wrote {len(rules)} rules to {args.out}")
+    old = {}
+    if os.path.exists(args.out):
+        with open(args.out) as f:
+            old = json.load(f)
+    rules, meta = old.get("rules", []), old.get("meta", {})
+    batch = old.get("batch")
+    if args.what in ("all", "single"):
+        buckets = [b for b in DEFAULT_BUCKETS if b[0] <= args.max_rows]
+        rules, meta = tune(buckets, args.steps, verbose=True)
+        meta["device"] = name
+    if args.what in ("all", "batch"):
+        bt, binfo = tune_batch(steps=max(2, args.steps // 2), verbose=True)
+        batch = {**bt, "meta": {"device": name, "when": time.strftime("%Y-%m-%dT%H:%M:%S"), **binfo}}
+    with open(args.out, "w") as f:
+        json.dump({"rules": list(rules), "meta": meta, **({"batch": batch} if batch else {})}, f, indent=1)
+    print(f"wrote {len(rules)} rules{' and batch tuning' if batch else ''} to {args.out}")
 
 
 if __name__ == "__main__":

@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -27,8 +28,6 @@
 
 namespace gb {
 
-constexpr int kBatchThreads = 512;
-constexpr int64_t kBatchTile = 65536;
 constexpr int kSampleRows = 2048;
 constexpr int kSampleSlots = 4096;
 
@@ -134,7 +133,8 @@ static __global__ void k_batch_init(uint8_t* T, int64_t nslots, int stride, cons
 // Aggregation of the tile list: one CTA per tile (largest instances first), so
 // that kernels of other streams (the serving loop's sketch) interleave at tile
 // granularity.
-static __global__ void __launch_bounds__(kBatchThreads) k_batch_aggregate(const __grid_constant__ Plan P,
+template <int NT>
+static __global__ void __launch_bounds__(NT) k_batch_aggregate(const __grid_constant__ Plan P,
                                                                           const BatchInst* insts,
                                                                           const BatchTile* tiles, int64_t ntiles,
                                                                           unsigned int* work,
@@ -347,6 +347,7 @@ struct Batch::Impl {
   SlotTemplate tmpl;
   int smem_bytes = 0;
   int grid_agg = 0, grid_compact = 0;
+  int block = 512;
   int64_t total_slots = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -448,14 +449,31 @@ struct Batch::Impl {
     if (h_counters) cudaFreeHost(h_counters);
   }
 
+  template <int NT>
+  void launch_agg(cudaStream_t s)
+  {
+    k_batch_aggregate<NT><<<grid_agg, NT, smem_bytes, s>>>(P, (const BatchInst*)d_insts.p, (const BatchTile*)d_tiles.p,
+                                                           (int64_t)tiles.size(), (unsigned int*)d_work.p, tmpl);
+  }
+  static const void* agg_kernel(int block)
+  {
+    switch (block) {
+      case 256: return (const void*)k_batch_aggregate<256>;
+      case 1024: return (const void*)k_batch_aggregate<1024>;
+      default: return (const void*)k_batch_aggregate<512>;
+    }
+  }
+
   void enqueue(cudaStream_t s)
   {
     ck(cudaMemsetAsync(d_counters.p, 0, (size_t)ninst * counter_words * 4, s), "memset counters");
     ck(cudaMemsetAsync(d_work.p, 0, 16, s), "memset work");
     k_batch_init<<<sms * 8, 256, 0, s>>>((uint8_t*)d_tables.p, total_slots, P.slot_bytes, tmpl);
-    k_batch_aggregate<<<grid_agg, kBatchThreads, smem_bytes, s>>>(P, (const BatchInst*)d_insts.p,
-                                                                  (const BatchTile*)d_tiles.p, (int64_t)tiles.size(),
-                                                                  (unsigned int*)d_work.p, tmpl);
+    switch (block) {
+      case 256: launch_agg<256>(s); break;
+      case 1024: launch_agg<1024>(s); break;
+      default: launch_agg<512>(s); break;
+    }
     k_batch_finish<<<(ninst + 255) / 256, 256, 0, s>>>(P, (const BatchInst*)d_insts.p, ninst);
     // output masks start at zero (compaction ORs bits in)
     if (mask_end > mask_begin)
@@ -521,11 +539,31 @@ std::vector<int64_t> batch_estimate_groups(const std::vector<std::vector<Column>
 Batch::Batch() : impl(new Impl) {}
 Batch::~Batch() = default;
 
+namespace {
+std::mutex g_batch_mu;
+std::vector<BatchRule> g_batch_rules;
+BatchLaunch g_batch_launch;
+}  // namespace
+
+void set_batch_tuning(const std::vector<BatchRule>& rules, const BatchLaunch& launch)
+{
+  std::lock_guard<std::mutex> lk(g_batch_mu);
+  g_batch_rules = rules;
+  g_batch_launch = launch;
+}
+
 void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_policy,
                     const std::vector<std::vector<Request>>& reqs, cudaStream_t stream, const Allocator& A,
                     const BatchOptions& bo)
 {
   Impl& B = *impl;
+  std::vector<BatchRule> rules;
+  BatchLaunch launch;
+  {
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    rules = g_batch_rules;
+    launch = g_batch_launch;
+  }
   const int ninst = (int)keys.size();
   if (ninst < 1) throw Error(ERR_LOGIC, "a batch needs at least one instance");
   if (reqs.size() != keys.size()) throw Error(ERR_LOGIC, "one request list per instance is required");
@@ -613,7 +651,7 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
   const int stride = B.P.slot_bytes;
   int scap_max = 1;
   {
-    int budget = std::min(bo.smem_bytes, optin - 8192 - (int)sizeof(Plan));
+    int budget = std::min(bo.smem_bytes >= 0 ? bo.smem_bytes : launch.smem_bytes, optin - 8192 - (int)sizeof(Plan));
     while ((int64_t)scap_max * 2 * stride <= budget) scap_max *= 2;
     if (scap_max * stride > budget) scap_max = 0;
   }
@@ -637,10 +675,21 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
     cap = std::max<uint64_t>(cap, 64);
     B.caps[i] = (int64_t)cap;
     // shared-memory stage only when the instance's groups fit a tile's table
+    // (a tuning rule of the instance's size bucket may cap the table or turn
+    // the stage off)
+    int slots_cap = scap_max;
+    double headroom = 2.0;
+    for (const BatchRule& r : rules) {
+      if (n > r.max_rows || (int64_t)est > r.max_groups) continue;
+      if (r.smem_slots >= 0) slots_cap = std::min(slots_cap, r.smem_slots);
+      if (r.headroom > 0) headroom = r.headroom;
+      ++B.stats.ruled_instances;
+      break;
+    }
     int sc = 0;
-    if (scap_max >= 64 && est * 2 <= scap_max && n > 4096) {
+    if (slots_cap >= 64 && est * headroom <= slots_cap && n > 4096) {
       sc = 64;
-      while (sc < scap_max && sc < est * 4) sc *= 2;
+      while (sc < slots_cap && sc < est * 2 * headroom) sc *= 2;
     }
     B.insts[i].scap = sc;
     B.insts[i].sfill = std::max(1, sc / 2);
@@ -649,14 +698,14 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
   }
   B.d_counters.get(A, (size_t)ninst * B.counter_words * 4, stream);
   B.d_work.get(A, 16, stream);
-  // tiles: instances cut into kBatchTile-row pieces, largest first
+  // tiles: instances cut into tile_rows-row pieces, largest first
   std::vector<int> order(ninst);
   for (int i = 0; i < ninst; ++i) order[i] = i;
   std::sort(order.begin(), order.end(), [&](int a, int b) { return B.insts[a].n_rows > B.insts[b].n_rows; });
   B.tiles.clear();
   for (int i : order)
-    for (int64_t b = 0; b < B.insts[i].n_rows; b += kBatchTile)
-      B.tiles.push_back(BatchTile{i, 0, b, std::min(B.insts[i].n_rows, b + kBatchTile)});
+    for (int64_t b = 0; b < B.insts[i].n_rows; b += launch.tile_rows)
+      B.tiles.push_back(BatchTile{i, 0, b, std::min(B.insts[i].n_rows, b + launch.tile_rows)});
   B.d_tiles.get(A, sizeof(BatchTile) * std::max<size_t>(1, B.tiles.size()), stream);
   if (!B.tiles.empty())
     ck(cudaMemcpyAsync(B.d_tiles.p, B.tiles.data(), sizeof(BatchTile) * B.tiles.size(), cudaMemcpyHostToDevice, stream),
@@ -664,9 +713,12 @@ void Batch::prepare(const std::vector<std::vector<Column>>& keys, int null_polic
   if (!B.h_counters) ck(cudaMallocHost((void**)&B.h_counters, (size_t)ninst * B.counter_words * 4), "cudaMallocHost");
   // launch shapes
   B.smem_bytes = scap_max * stride;
-  allow_max_smem((const void*)k_batch_aggregate);
+  B.block = launch.block;
+  B.stats.block = launch.block;
+  B.stats.tile_rows = launch.tile_rows;
+  allow_max_smem(Impl::agg_kernel(B.block));
   int bps = 0;
-  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_aggregate, kBatchThreads, B.smem_bytes), "occ");
+  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, Impl::agg_kernel(B.block), B.block, B.smem_bytes), "occ");
   B.grid_agg = (int)std::min<int64_t>(std::max<int64_t>(1, (int64_t)B.tiles.size()), 1 << 30);
   B.grid_compact = sms * 8;
   B.stats.instances = ninst;
@@ -899,6 +951,31 @@ int gb_batch_get_stats(const gb_batch* b, gb_batch_stats* out)
     out->output_bytes = s.output_bytes;
     out->kernels_per_run = s.kernels_per_run;
     out->regrown = s.regrown;
+    out->block = s.block;
+    out->tile_rows = s.tile_rows;
+    out->ruled_instances = s.ruled_instances;
+  });
+}
+
+int gb_batch_set_tuning(const gb_batch_rule* rules, int32_t num_rules, const gb_batch_launch* launch)
+{
+  return guarded([&] {
+    if (num_rules < 0 || (num_rules > 0 && !rules)) throw gb::Error(gb::ERR_LOGIC, "bad batch tuning rules");
+    gb::BatchLaunch L;
+    if (launch) {
+      if (launch->block != 256 && launch->block != 512 && launch->block != 1024)
+        throw gb::Error(gb::ERR_LOGIC, "batch block must be 256, 512 or 1024");
+      if (launch->tile_rows < 1024) throw gb::Error(gb::ERR_LOGIC, "batch tile_rows must be >= 1024");
+      if (launch->smem_bytes < 0) throw gb::Error(gb::ERR_LOGIC, "batch smem_bytes must be >= 0");
+      L.block = launch->block;
+      L.tile_rows = launch->tile_rows;
+      L.smem_bytes = launch->smem_bytes;
+    }
+    std::vector<gb::BatchRule> v;
+    for (int i = 0; i < num_rules; ++i)
+      v.push_back(gb::BatchRule{rules[i].max_rows, rules[i].max_groups, rules[i].smem_slots,
+                                rules[i].headroom_pct > 0 ? rules[i].headroom_pct / 100.0 : -1.0});
+    gb::set_batch_tuning(v, L);
   });
 }
 

@@ -7,9 +7,28 @@
 
 namespace gb {
 
+// Batch tuning (an autotuner picks these; see cudf_b200.autotune):
+//  launch-wide: threads per CTA of the aggregation kernel (256, 512 or 1024),
+//  rows per tile, and the shared-memory budget of a tile's table;
+//  per instance, by the first rule with rows <= max_rows and estimated
+//  groups <= max_groups: at most smem_slots shared slots (0: the global table
+//  only) and the shared stage only when groups * headroom <= slots.
+struct BatchRule {
+  int64_t max_rows;
+  int64_t max_groups;
+  int smem_slots;    // -1: unset
+  double headroom;   // <= 0: unset
+};
+struct BatchLaunch {
+  int block = 512;
+  int64_t tile_rows = 65536;
+  int smem_bytes = 160 * 1024;
+};
+void set_batch_tuning(const std::vector<BatchRule>& rules, const BatchLaunch& launch);
+
 struct BatchOptions {
   bool use_graph = false;  // capture the run sequence once, replay it
-  int smem_bytes = 160 * 1024;
+  int smem_bytes = -1;     // shared-memory budget of a tile's table (-1: the tuned launch's)
   double growth = 1.0;     // multiplies every instance's group estimate (tables size from it)
   bool trial = true;       // run once at prepare time and regrow overflowing / overfull tables
   std::vector<int64_t> est_groups;  // per-instance estimates from the caller (skips sampling)
@@ -27,6 +46,9 @@ struct BatchStats {
   int trial_rounds = 0;
   double sample_s = 0, layout_s = 0, trial_s = 0, run_s = 0;
   int kernels_per_run = 0;
+  int block = 0;             // launch used
+  int64_t tile_rows = 0;
+  int64_t ruled_instances = 0;  // instances a tuning rule sized
 };
 
 // Device-side key sketch: estimated group count of each instance (one

@@ -233,6 +233,9 @@ typedef struct gb_batch_stats {
   int64_t output_bytes;
   int32_t kernels_per_run;
   int64_t regrown;          /* instance tables grown after a trial run overflowed */
+  int32_t block;            /* threads per CTA of the aggregation launch */
+  int64_t tile_rows;        /* rows per tile of the work queue */
+  int64_t ruled_instances;  /* instances a gb_batch_rule sized */
 } gb_batch_stats;
 GB_API int gb_batch_prepare(int32_t num_instances, const gb_column* keys, int32_t num_keys,
                             int32_t null_policy, const gb_request* requests, int32_t num_requests,
@@ -242,6 +245,29 @@ GB_API int gb_batch_result(gb_batch* batch, int32_t instance, int64_t* num_group
                            gb_out_column* keys, gb_out_column* results);
 GB_API int gb_batch_get_stats(const gb_batch* batch, gb_batch_stats* out);
 GB_API void gb_batch_destroy(gb_batch* batch);
+
+/* Process-wide tuning of batched launches (no counterpart in libcudf).
+ * launch (NULL: defaults 512 threads, 64 Ki-row tiles, 160 KiB tables): the
+ * aggregation kernel's threads per CTA (256, 512 or 1024), rows per tile of
+ * the work queue, shared-memory bytes of a tile's table.  rules: for each
+ * instance, the first rule with rows <= max_rows and estimated groups <=
+ * max_groups caps its shared table at smem_slots slots (0: global table
+ * only; -1: no cap) and takes the shared stage only when groups *
+ * headroom_pct / 100 <= slots (<= 0: 200).  Applies to batches prepared
+ * afterwards; replaces earlier settings.  cudf_b200.autotune times the
+ * candidates per size bucket. */
+typedef struct gb_batch_rule {
+  int64_t max_rows;
+  int64_t max_groups;
+  int32_t smem_slots;
+  int32_t headroom_pct;
+} gb_batch_rule;
+typedef struct gb_batch_launch {
+  int32_t block;
+  int32_t tile_rows;
+  int32_t smem_bytes;
+} gb_batch_launch;
+GB_API int gb_batch_set_tuning(const gb_batch_rule* rules, int32_t num_rules, const gb_batch_launch* launch);
 
 /* Serving loop: continuous batching of groupby queries (no counterpart in
  * libcudf).  gb_server_submit enqueues a query whose columns are resident on

@@ -31,3 +31,14 @@ def test_invalid_rule_is_rejected():
 def test_tuning_struct_defaults_are_unset():
     t = autotune._tuning_struct({"scatter": 2})
     assert t.scatter == 2 and t.force_mode == -2 and t.block == -1 and t.smem_bytes == -1
+
+
+def test_batch_tuning_install_and_reject():
+    autotune.set_batch_tuning([{"max_rows": 1 << 20, "max_groups": 1 << 10, "headroom_pct": 300},
+                               {"max_rows": 1 << 30, "max_groups": 1 << 30, "smem_slots": 0}],
+                              {"block": 256, "tile_rows": 16384, "smem_bytes": 96 * 1024})
+    with pytest.raises(ValueError):
+        autotune.set_batch_tuning([], {"block": 300, "tile_rows": 16384, "smem_bytes": 0})
+    with pytest.raises(ValueError):
+        autotune.set_batch_tuning([], {"block": 512, "tile_rows": 10, "smem_bytes": 0})
+    autotune.set_batch_tuning([], autotune.BATCH_LAUNCH_DEFAULT)

@@ -74,7 +74,18 @@ def test_batch_two_word_keys_include_nulls():
     _run(_instances(8, 12, max_rows=50_000, max_card=2_000, two_keys=True), True, True)
 
 
-def test_batch_low_cardinality_uses_shared_tables():
+@pytest.fixture
+def default_batch_tuning():
+    """Batches prepared inside the test use the built-in launch and no rules
+    (the shipped tuning file may set others); the shipped tuning is put back."""
+    from cudf_b200 import autotune
+    autotune.set_batch_tuning([], autotune.BATCH_LAUNCH_DEFAULT)
+    yield autotune
+    autotune.set_batch_tuning([], autotune.BATCH_LAUNCH_DEFAULT)
+    autotune.load()
+
+
+def test_batch_low_cardinality_uses_shared_tables(default_batch_tuning):
     rng = np.random.default_rng(9)
     inst = []
     for card in (1, 2, 4, 8, 100):
@@ -93,3 +104,18 @@ def test_batch_rejects_mixed_schemas():
     v = cb.Column.from_numpy(np.arange(10, dtype=np.int64))
     with pytest.raises(ValueError):
         cb.BatchGroupBy([(a, [cb.GroupByRequest(v, [agg.sum()])]), (b, [cb.GroupByRequest(v, [agg.sum()])])])
+
+
+@pytest.mark.parametrize("launch", [{"block": 256, "tile_rows": 4096, "smem_bytes": 96 * 1024},
+                                    {"block": 1024, "tile_rows": 262144, "smem_bytes": 200 * 1024}])
+def test_batch_tuned_launch_and_rules_match_oracle(default_batch_tuning, launch):
+    """Other block sizes and tile lengths, and per-instance rules that send
+    one size bucket to the global table and give another more headroom."""
+    autotune = default_batch_tuning
+    rules = [{"max_rows": 20_000, "max_groups": 1 << 30, "smem_slots": 0},
+             {"max_rows": 1 << 30, "max_groups": 2_000, "headroom_pct": 400}]
+    autotune.set_batch_tuning(rules, launch)
+    bg = _run(_instances(10, 24), True, False, replays=1)
+    st = bg.stats()
+    assert st["block"] == launch["block"] and st["tile_rows"] == launch["tile_rows"]
+    assert st["ruled_instances"] >= 1
