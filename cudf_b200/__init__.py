@@ -9,6 +9,7 @@ from .groupby import GroupBy, GroupByRequest
 from .serving import Server
 from .types import Kind, NullPolicy, Sorted, TypeId
 from .frame import DataFrame
+from .io import groupby_parquet, read_parquet, scan_parquet
 
 def _install_tuning():
     """Installs the measured per-size-bucket tuning rules shipped with the
@@ -25,5 +26,5 @@ def _install_tuning():
 _install_tuning()
 
 __all__ = ["aggregation", "BatchGroupBy", "Column", "DataFrame", "HostStaging", "Table", "GroupBy", "GroupByRequest",
-           "Kind", "NullPolicy", "Server", "Sorted", "TypeId"]
+           "Kind", "NullPolicy", "Server", "Sorted", "TypeId", "groupby_parquet", "read_parquet", "scan_parquet"]
 __version__ = "0.1.0"

@@ -126,6 +126,83 @@ def engine_local_aggregate(keys, requests, null_handling):
     return out_keys, out_res
 
 
+def plan_partials(requests):
+    """The partial aggregations each request needs (MEAN -> SUM + COUNT_VALID,
+    every other kind itself), without repeats: [(col, [Kind])]."""
+    preq = []
+    for (col, kinds) in requests:
+        plist = []
+        for k in kinds:
+            k = Kind(k)
+            if k not in _PARTIALS:
+                raise NotImplementedError(f"{k.name} does not decompose into mergeable partials")
+            for p in _PARTIALS[k]:
+                if p not in plist:
+                    plist.append(p)
+        preq.append((col, plist))
+    return preq
+
+
+def _partial_tid(col_tid: int, p: Kind, data: torch.Tensor) -> int:
+    """Type id of a partial column (counts merged once are int64 sums)."""
+    if p in (Kind.COUNT_VALID, Kind.COUNT_ALL) and data.dtype == torch.int64:
+        return TypeId.INT64
+    return _partial_type(col_tid, p)
+
+
+def merge_partials(preq, pkeys, pvals, null_handling, local):
+    """Merges partial groups (the same key may appear in several rows) with a
+    second groupby: SUM of sums and counts, MIN of mins, MAX of maxes, PRODUCT
+    of products.  pkeys: [(data, valid, type_id)]; pvals[(r, j)] = (data,
+    valid) of partial j of request r.  Returns (keys, merged) with
+    merged[r][kind] = (data, valid) -- again partials, ready to merge again
+    or to finalize."""
+    mreq = []
+    for r, (col, plist) in enumerate(preq):
+        for j, p in enumerate(plist):
+            d, v = pvals[(r, j)]
+            mreq.append(((d, v, _partial_tid(col[2], p, d)), [_MERGE[p]]))
+    policy = NullPolicy.INCLUDE if null_handling == NullPolicy.INCLUDE else NullPolicy.EXCLUDE
+    mk, mres = local(pkeys, mreq, policy)
+    merged, i = [], 0
+    for r, (col, plist) in enumerate(preq):
+        per = {}
+        for p in plist:
+            per[p] = mres[i][0]
+            i += 1
+        merged.append(per)
+    return mk, merged
+
+
+def finalize_partials(requests, merged):
+    """Results in request order from merged partials: MEAN = SUM / COUNT in
+    double (durations: integer mean), counts as int32, the rest as merged."""
+    out = []
+    for r, (col, kinds) in enumerate(requests):
+        per = []
+        for k in kinds:
+            k = Kind(k)
+            if k == Kind.MEAN:
+                s, sv = merged[r][Kind.SUM]
+                c, _ = merged[r][Kind.COUNT_VALID]
+                c = c.to(torch.int64)
+                valid = c > 0
+                if col[2] in _DURATIONS:
+                    mean = torch.where(valid, torch.div(s.to(torch.int64), c.clamp(min=1), rounding_mode="trunc"),
+                                       torch.zeros_like(s, dtype=torch.int64)).to(s.dtype)
+                else:
+                    mean = torch.where(valid, s.to(torch.float64) / c.clamp(min=1).to(torch.float64),
+                                       torch.zeros_like(s, dtype=torch.float64))
+                per.append((mean, valid if (sv is not None or col[1] is not None) else None))
+            elif k in (Kind.COUNT_VALID, Kind.COUNT_ALL):
+                d, _ = merged[r][k]
+                per.append((d.to(torch.int32), None))
+            else:
+                per.append(merged[r][k])
+        out.append(per)
+    return out
+
+
 def distributed_groupby(keys, requests, null_handling: NullPolicy = NullPolicy.EXCLUDE, group=None,
                         local_aggregate: Optional[Callable] = None):
     """keys: [(data, valid|None, type_id)] of this rank's shard; requests:
@@ -134,18 +211,7 @@ def distributed_groupby(keys, requests, null_handling: NullPolicy = NullPolicy.E
     local = local_aggregate or engine_local_aggregate
     world = dist.get_world_size(group)
     # 1. partial aggregation of the shard
-    preq, slots = [], []
-    for (col, kinds) in requests:
-        plist = []
-        for k in kinds:
-            k = Kind(k)
-            if k not in _PARTIALS:
-                raise NotImplementedError(f"{k.name} is not supported by the multi-GPU groupby")
-            for p in _PARTIALS[k]:
-                if p not in plist:
-                    plist.append(p)
-        preq.append((col, plist))
-        slots.append(plist)
+    preq = plan_partials(requests)
     pk, pres = local(keys, preq, null_handling)
     # 2. route every partial group to the rank owning its key
     dest = owner_rank([(d, v, t) for d, v, t in pk], world)
@@ -171,47 +237,9 @@ def distributed_groupby(keys, requests, null_handling: NullPolicy = NullPolicy.E
             rkeys.append((d, v, info))
         else:
             rvals[info] = (d, v)
-    # 3. merge the partials this rank owns
-    mreq = []
-    for r, (col, plist) in enumerate(preq):
-        for j, p in enumerate(plist):
-            d, v = rvals[(r, j)]
-            tid = _partial_type(col[2], p)
-            mreq.append(((d, v, tid), [_MERGE[p]]))
-    policy = NullPolicy.INCLUDE if null_handling == NullPolicy.INCLUDE else NullPolicy.EXCLUDE
-    mk, mres = local(rkeys, mreq, policy)
-    merged, i = [], 0
-    for r, (col, plist) in enumerate(preq):
-        per = {}
-        for p in plist:
-            per[p] = mres[i][0]
-            i += 1
-        merged.append(per)
-    # 4. finalize in request order
-    out = []
-    for r, (col, kinds) in enumerate(requests):
-        per = []
-        for k in kinds:
-            k = Kind(k)
-            if k == Kind.MEAN:
-                s, sv = merged[r][Kind.SUM]
-                c, _ = merged[r][Kind.COUNT_VALID]
-                c = c.to(torch.int64)
-                valid = c > 0
-                if col[2] in _DURATIONS:
-                    mean = torch.where(valid, torch.div(s.to(torch.int64), c.clamp(min=1), rounding_mode="trunc"),
-                                       torch.zeros_like(s, dtype=torch.int64)).to(s.dtype)
-                else:
-                    mean = torch.where(valid, s.to(torch.float64) / c.clamp(min=1).to(torch.float64),
-                                       torch.zeros_like(s, dtype=torch.float64))
-                per.append((mean, valid if (sv is not None or col[1] is not None) else None))
-            elif k in (Kind.COUNT_VALID, Kind.COUNT_ALL):
-                d, _ = merged[r][k]
-                per.append((d.to(torch.int32), None))
-            else:
-                per.append(merged[r][k])
-        out.append(per)
-    return mk, out
+    # 3. merge the partials this rank owns; 4. finalize in request order
+    mk, merged = merge_partials(preq, rkeys, rvals, null_handling, local)
+    return mk, finalize_partials(requests, merged)
 
 
 def _partial_type(tid: int, p: Kind) -> int:
