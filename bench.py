@@ -601,84 +601,99 @@ def run_serve(args):
         m2 = pack_mask(torch.rand(pool_n, device=dev, generator=g) >= 0.1)
         pool.append((k, v1, v2, m1, m2))
     torch.cuda.synchronize()
-    nq = int(rng.poisson(args.rate * args.duration))
-    arrivals = np.sort(rng.uniform(0, args.duration, nq))
-    which = rng.integers(0, args.pool, nq)
-    rows = np.exp(rng.uniform(np.log(1e4), np.log(2e7), nq)).astype(np.int64)
 
-    def query(i):
-        k, v1, v2, m1, m2 = pool[which[i]]
-        n = int(rows[i])
-        kt = cb.Table([cb.Column(TypeId.INT64, k, size=n)])
-        aggs = [agg.sum(), agg.count(), agg.mean()]
-        return kt, [cb.GroupByRequest(cb.Column(TypeId.INT64, v1, m1, size=n), aggs),
-                    cb.GroupByRequest(cb.Column(TypeId.FLOAT64, v2, m2, size=n), aggs)]
+    def one_stream(rate):
+        nq = int(rng.poisson(rate * args.duration))
+        arrivals = np.sort(rng.uniform(0, args.duration, nq))
+        which = rng.integers(0, args.pool, nq)
+        rows = np.exp(rng.uniform(np.log(1e4), np.log(2e7), nq)).astype(np.int64)
 
-    qs = [query(i) for i in range(nq)]
-    # plain single-query latency (no queueing): a sample of queries run alone
-    for i in range(5):
-        cb.GroupBy(qs[i][0]).aggregate(qs[i][1])
-    alone = []
-    for i in range(min(nq, 200)):
-        t = time.perf_counter()
-        cb.GroupBy(qs[i][0]).aggregate(qs[i][1])
-        alone.append(time.perf_counter() - t)
-    alone_p50 = float(np.median(alone))
+        def query(i):
+            k, v1, v2, m1, m2 = pool[which[i]]
+            n = int(rows[i])
+            kt = cb.Table([cb.Column(TypeId.INT64, k, size=n)])
+            aggs = [agg.sum(), agg.count(), agg.mean()]
+            return kt, [cb.GroupByRequest(cb.Column(TypeId.INT64, v1, m1, size=n), aggs),
+                        cb.GroupByRequest(cb.Column(TypeId.FLOAT64, v2, m2, size=n), aggs)]
 
-    def plain():
-        lat = []
-        t0 = time.perf_counter()
-        for i in range(nq):
-            now = time.perf_counter() - t0
-            if now < arrivals[i]:
-                time.sleep(arrivals[i] - now)
+        qs = [query(i) for i in range(nq)]
+        # plain single-query latency (no queueing): a sample of queries run alone
+        for i in range(5):
             cb.GroupBy(qs[i][0]).aggregate(qs[i][1])
-            lat.append(time.perf_counter() - t0 - arrivals[i])
-        span = time.perf_counter() - t0
-        return {"queries_per_s": nq / span, "p50_s": float(np.percentile(lat, 50)),
-                "p99_s": float(np.percentile(lat, 99)), "completed": nq}
+        alone = []
+        for i in range(min(nq, 200)):
+            t = time.perf_counter()
+            cb.GroupBy(qs[i][0]).aggregate(qs[i][1])
+            alone.append(time.perf_counter() - t)
+        alone_p50 = float(np.median(alone))
 
-    def batched():
-        srv = cb.Server(memory_cap_bytes=150 << 30, workers=args.workers, direct_rows=args.direct_rows)
-        ids = [None] * nq
-        done = threading.Event()
-
-        def collector():
-            for i in range(nq):
-                while ids[i] is None:
-                    time.sleep(1e-4)
-                srv.wait(ids[i], timeout_s=600)
-                srv.release(ids[i])
-            done.set()
-
-        th = threading.Thread(target=collector)
-        th.start()
-        try:
+        def plain():
+            lat = []
             t0 = time.perf_counter()
             for i in range(nq):
                 now = time.perf_counter() - t0
                 if now < arrivals[i]:
                     time.sleep(arrivals[i] - now)
-                ids[i] = srv.submit(*qs[i])
-            th.join()
-            return srv.stats()
-        finally:
-            srv.close()
+                cb.GroupBy(qs[i][0]).aggregate(qs[i][1])
+                lat.append(time.perf_counter() - t0 - arrivals[i])
+            span = time.perf_counter() - t0
+            return {"queries_per_s": nq / span, "p50_s": float(np.percentile(lat, 50)),
+                    "p99_s": float(np.percentile(lat, 99)), "completed": nq}
 
-    b = batched()
-    p = plain()
-    line = {"metric": f"served groupby queries/s (Poisson {args.rate}/s for {args.duration}s)",
-            "value": b["queries_per_s"], "unit": "queries/s", "n_gpus": 1, "steps": 1, "warmup": 0,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64",
-            "data": "synthetic",
-            "config": {"workload": "serving stream: int64 keys (cardinality log-uniform [10,1e6]), rows "
-                                   "log-uniform [1e4,2e7], int64+f64 values 10% nulls, sum/count/mean, "
-                                   "admission cap 150 GB", "queries": nq, "rate": args.rate,
-                       "duration_s": args.duration, "pool_tables": args.pool, "workers": args.workers,
-                       "mean_rows": float(rows.mean())},
-            "batched": b, "plain": p, "plain_single_query_latency_s": alone_p50,
-            "qps_ratio_vs_plain": b["queries_per_s"] / p["queries_per_s"],
-            "p99_over_plain_single": b["p99_s"] / alone_p50}
+        def batched():
+            srv = cb.Server(memory_cap_bytes=150 << 30, workers=args.workers, direct_rows=args.direct_rows)
+            ids = [None] * nq
+            done = threading.Event()
+
+            def collector():
+                for i in range(nq):
+                    while ids[i] is None:
+                        time.sleep(1e-4)
+                    srv.wait(ids[i], timeout_s=600)
+                    srv.release(ids[i])
+                done.set()
+
+            th = threading.Thread(target=collector)
+            th.start()
+            try:
+                t0 = time.perf_counter()
+                for i in range(nq):
+                    now = time.perf_counter() - t0
+                    if now < arrivals[i]:
+                        time.sleep(arrivals[i] - now)
+                    ids[i] = srv.submit(*qs[i])
+                th.join()
+                return srv.stats()
+            finally:
+                srv.close()
+
+        b = batched()
+        p = plain()
+        line = {"metric": f"served groupby queries/s (Poisson {rate}/s for {args.duration}s)",
+                "value": b["queries_per_s"], "unit": "queries/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64",
+                "data": "synthetic",
+                "config": {"workload": "serving stream: int64 keys (cardinality log-uniform [10,1e6]), rows "
+                                       "log-uniform [1e4,2e7], int64+f64 values 10% nulls, sum/count/mean, "
+                                       "admission cap 150 GB", "queries": nq, "rate": rate,
+                           "duration_s": args.duration, "pool_tables": args.pool, "workers": args.workers,
+                           "mean_rows": float(rows.mean())},
+                "batched": b, "plain": p, "plain_single_query_latency_s": alone_p50,
+                "qps_ratio_vs_plain": b["queries_per_s"] / p["queries_per_s"],
+                "p99_over_plain_single": b["p99_s"] / alone_p50}
+        return line
+
+    rates = [float(r) for r in args.rates.split(",")] if args.rates else [args.rate]
+    lines = [one_stream(r) for r in rates]
+    line = lines[0]
+    if len(lines) > 1:
+        # offered-rate curve: where the plain loop saturates and what the
+        # server delivers there
+        line["curve"] = [{"offered_qps": r, "batched_qps": l["batched"]["queries_per_s"],
+                          "plain_qps": l["plain"]["queries_per_s"], "qps_ratio_vs_plain": l["qps_ratio_vs_plain"],
+                          "batched_p99_s": l["batched"]["p99_s"], "plain_p99_s": l["plain"]["p99_s"],
+                          "p99_over_plain_single": l["p99_over_plain_single"], "queries": l["config"]["queries"]}
+                         for r, l in zip(rates, lines)]
     return line
 
 
@@ -912,6 +927,7 @@ def main():
     ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "zipf", "small"])
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--rate", type=float, default=2000.0)
+    ap.add_argument("--rates", default="", help="serve: comma-separated offered rates (a curve); first is the line's")
     ap.add_argument("--duration", type=float, default=5.0)
     ap.add_argument("--pool", type=int, default=16)
     ap.add_argument("--workers", type=int, default=4)
