@@ -173,9 +173,13 @@ struct RunAcc {
       }
     }
   }
-  // order-preserving encodings of the slot's MIN/MAX fields
+  // order-preserving encodings of the slot's MIN/MAX fields; a run without
+  // valid values gives the field's identity (all ones for MIN, zero for MAX:
+  // the register extremes of a narrow signed type would truncate to real
+  // encodings)
   __device__ __forceinline__ uint64_t enc_min() const
   {
+    if (nvalid == 0) return W == 8 ? ~0ull : 0xFFFFFFFFull;
     if (CAT == CAT_F64) return ord64_f(mn, true);
     if (CAT == CAT_F32) return ord32_f(mn, true);
     if (CAT == CAT_SIGNED) return W == 8 ? ((uint64_t)mn ^ 0x8000000000000000ull) : ((uint32_t)(int32_t)(int64_t)mn ^ 0x80000000u);
@@ -183,6 +187,7 @@ struct RunAcc {
   }
   __device__ __forceinline__ uint64_t enc_max() const
   {
+    if (nvalid == 0) return 0;
     if (CAT == CAT_F64) return ord64_f(mx, false);
     if (CAT == CAT_F32) return ord32_f(mx, false);
     if (CAT == CAT_SIGNED) return W == 8 ? ((uint64_t)mx ^ 0x8000000000000000ull) : ((uint32_t)(int32_t)(int64_t)mx ^ 0x80000000u);

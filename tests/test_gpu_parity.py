@@ -208,7 +208,7 @@ def test_config_shapes_medium(n, card, nulls):
               (cb.Column.from_numpy(v3, masks[2]), aggs)])
 
 
-@pytest.mark.parametrize("scatter", [0, 1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("scatter", [0, 1, 2, 3, 4, 5, 6, 7])
 @pytest.mark.parametrize("nulls", [False, True])
 @pytest.mark.parametrize("two_word", [False, True])
 def test_partitioned_mode(nulls, two_word, scatter):
