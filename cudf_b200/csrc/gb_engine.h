@@ -77,8 +77,8 @@ struct Options {
   int64_t groups_hint = -1;    // caller's group-count estimate (-1: sample)
   int force_mode = -1;         // -1 auto, 0 global only, 1 smem stage
   int profile = 0;             // time kernels with CUDA events
-  int scatter = 7;             // partitioned pass 1: 7 bulk-copy tiles where the columns allow, else 0-6 (launch shapes)
-  int pass2 = 0;               // partitioned pass 2: 0 sorted 512x4, 1 per-row reductions, 2 sorted 1024x2, 3 sorted 256x8
+  int scatter = 0;             // partitioned pass 1: 0-6 launch shapes of the per-thread scatter, 7 bulk-copy tiles
+  int pass2 = 1;               // partitioned pass 2: 1 per-row shared reductions, 0/2 sorted chunks 512x4, 3 sorted 256x8
   uint32_t set_mask = 0;       // OPT_* bits of the fields a caller set explicitly
   // internal: 0 reads every outcome (group counts, overflow flags, null
   // counts) back once, after the compaction, sizing the outputs by an upper

@@ -401,6 +401,17 @@ __device__ __forceinline__ uint64_t sld_u64(uint32_t a)
   return v;
 }
 
+// MIN/MAX updates that skip the shared reduction when a plain read of the
+// field shows the value cannot change it.  A MIN field only decreases and a
+// MAX field only increases, so a stale read can let a useless update through
+// but never drops a needed one; on this architecture the 64-bit reductions
+// are compare-and-swap loops, and after a group's first rows most values no
+// longer improve its MIN or MAX.
+__device__ __forceinline__ void smin_u64(uint32_t a, uint64_t v) { if (v < sld_u64(a)) sred_min_u64(a, v); }
+__device__ __forceinline__ void smax_u64(uint32_t a, uint64_t v) { if (v > sld_u64(a)) sred_max_u64(a, v); }
+__device__ __forceinline__ void smin_u32(uint32_t a, uint32_t v) { if (v < sld_u32(a)) sred_min_u32(a, v); }
+__device__ __forceinline__ void smax_u32(uint32_t a, uint32_t v) { if (v > sld_u32(a)) sred_max_u32(a, v); }
+
 // Rows whose key did not fit their partition's shared table (a partition
 // with more groups than the sample predicted) are listed by pass 2 and
 // applied to the global spill table afterwards by k_part_spill, so the hot
@@ -569,14 +580,14 @@ __device__ __forceinline__ void p2_column(const ValCol& c, const uint32_t (&sa)[
       if (CAT == CAT_F64) {
         const double d = __longlong_as_double((long long)x[j]);
         if (so >= 0) { const double t = grp_reduce(grp, d, [](double p, double q) { return p + q; }); if (lead) sred_add_f64(a + so, t); }
-        if (mo >= 0) { const uint64_t t = grp_reduce(grp, ord64_f(d, true), min64); if (lead) sred_min_u64(a + mo, t); }
-        if (xo >= 0) { const uint64_t t = grp_reduce(grp, ord64_f(d, false), max64); if (lead) sred_max_u64(a + xo, t); }
+        if (mo >= 0) { const uint64_t t = grp_reduce(grp, ord64_f(d, true), min64); if (lead) smin_u64(a + mo, t); }
+        if (xo >= 0) { const uint64_t t = grp_reduce(grp, ord64_f(d, false), max64); if (lead) smax_u64(a + xo, t); }
         if (qo >= 0) { const double t = grp_reduce(grp, d * d, [](double p, double q) { return p + q; }); if (lead) sred_add_f64(a + qo, t); }
       } else if (CAT == CAT_F32) {
         const float f = __uint_as_float((uint32_t)x[j]);
         if (so >= 0) { const float t = grp_reduce(grp, f, [](float p, float q) { return p + q; }); if (lead) sred_add_f32(a + so, t); }
-        if (mo >= 0) { const uint32_t t = grp_reduce(grp, ord32_f(f, true), min32); if (lead) sred_min_u32(a + mo, t); }
-        if (xo >= 0) { const uint32_t t = grp_reduce(grp, ord32_f(f, false), max32); if (lead) sred_max_u32(a + xo, t); }
+        if (mo >= 0) { const uint32_t t = grp_reduce(grp, ord32_f(f, true), min32); if (lead) smin_u32(a + mo, t); }
+        if (xo >= 0) { const uint32_t t = grp_reduce(grp, ord32_f(f, false), max32); if (lead) smax_u32(a + xo, t); }
         if (qo >= 0) { const float t = grp_reduce(grp, f * f, [](float p, float q) { return p + q; }); if (lead) sred_add_f32(a + qo, t); }
       } else {
         int64_t iv;
@@ -593,12 +604,12 @@ __device__ __forceinline__ void p2_column(const ValCol& c, const uint32_t (&sa)[
         }
         if (W == 8) {
           const uint64_t o = CAT == CAT_SIGNED ? ((uint64_t)iv ^ 0x8000000000000000ull) : (uint64_t)iv;
-          if (mo >= 0) { const uint64_t t = grp_reduce(grp, o, min64); if (lead) sred_min_u64(a + mo, t); }
-          if (xo >= 0) { const uint64_t t = grp_reduce(grp, o, max64); if (lead) sred_max_u64(a + xo, t); }
+          if (mo >= 0) { const uint64_t t = grp_reduce(grp, o, min64); if (lead) smin_u64(a + mo, t); }
+          if (xo >= 0) { const uint64_t t = grp_reduce(grp, o, max64); if (lead) smax_u64(a + xo, t); }
         } else {
           const uint32_t o = CAT == CAT_SIGNED ? ((uint32_t)(int32_t)iv ^ 0x80000000u) : (uint32_t)iv;
-          if (mo >= 0) { const uint32_t t = grp_reduce(grp, o, min32); if (lead) sred_min_u32(a + mo, t); }
-          if (xo >= 0) { const uint32_t t = grp_reduce(grp, o, max32); if (lead) sred_max_u32(a + xo, t); }
+          if (mo >= 0) { const uint32_t t = grp_reduce(grp, o, min32); if (lead) smin_u32(a + mo, t); }
+          if (xo >= 0) { const uint32_t t = grp_reduce(grp, o, max32); if (lead) smax_u32(a + xo, t); }
         }
         if (qo >= 0) {
           const uint64_t t = grp_reduce(grp, (uint64_t)iv * (uint64_t)iv, add64);
@@ -614,14 +625,14 @@ __device__ __forceinline__ void p2_column(const ValCol& c, const uint32_t (&sa)[
     if (CAT == CAT_F64) {
       const double d = __longlong_as_double((long long)x[j]);
       if (so >= 0) sred_add_f64(a + so, d);
-      if (mo >= 0) sred_min_u64(a + mo, ord64_f(d, true));
-      if (xo >= 0) sred_max_u64(a + xo, ord64_f(d, false));
+      if (mo >= 0) smin_u64(a + mo, ord64_f(d, true));
+      if (xo >= 0) smax_u64(a + xo, ord64_f(d, false));
       if (qo >= 0) sred_add_f64(a + qo, d * d);
     } else if (CAT == CAT_F32) {
       const float f = __uint_as_float((uint32_t)x[j]);
       if (so >= 0) sred_add_f32(a + so, f);
-      if (mo >= 0) sred_min_u32(a + mo, ord32_f(f, true));
-      if (xo >= 0) sred_max_u32(a + xo, ord32_f(f, false));
+      if (mo >= 0) smin_u32(a + mo, ord32_f(f, true));
+      if (xo >= 0) smax_u32(a + xo, ord32_f(f, false));
       if (qo >= 0) sred_add_f32(a + qo, f * f);
     } else {
       // integers: sign- or zero-extended to 64 bits; min/max in the
@@ -637,12 +648,12 @@ __device__ __forceinline__ void p2_column(const ValCol& c, const uint32_t (&sa)[
       }
       if (W == 8) {
         const uint64_t o = CAT == CAT_SIGNED ? ((uint64_t)iv ^ 0x8000000000000000ull) : (uint64_t)iv;
-        if (mo >= 0) sred_min_u64(a + mo, o);
-        if (xo >= 0) sred_max_u64(a + xo, o);
+        if (mo >= 0) smin_u64(a + mo, o);
+        if (xo >= 0) smax_u64(a + xo, o);
       } else {
         const uint32_t o = CAT == CAT_SIGNED ? ((uint32_t)(int32_t)iv ^ 0x80000000u) : (uint32_t)iv;
-        if (mo >= 0) sred_min_u32(a + mo, o);
-        if (xo >= 0) sred_max_u32(a + xo, o);
+        if (mo >= 0) smin_u32(a + mo, o);
+        if (xo >= 0) smax_u32(a + xo, o);
       }
       if (qo >= 0) sred_add_u64(a + qo, (uint64_t)iv * (uint64_t)iv);
     }

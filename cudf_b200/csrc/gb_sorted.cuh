@@ -276,17 +276,27 @@ __device__ __forceinline__ uint64_t sum_bits(typename RunAcc<CAT, W>::S s)
   return (uint64_t)s;
 }
 
+// Where sorted position p of a chunk of R*NT rows is stored in the stage
+// arrays: thread-major (p % R) * NT + p / R, so that when thread t walks its
+// positions t*R .. t*R+R-1 the lanes of a warp touch consecutive elements
+// (no bank conflicts) instead of elements R apart.
+template <int R, int NT>
+__device__ __forceinline__ int stage_at(int p)
+{
+  return (p & (R - 1)) * NT + (p / R);
+}
+
 // The runs of thread t's positions [a, b) in the sorted chunk.  `cur` holds
 // the start of every slot's run (cur[s+1] is where run s ends).  Calls
 // fn(pos, len, slot, piece): a light run (at most L rows) whose start lies in
 // [a, b) is visited whole (piece = false; this thread is its only writer);
 // a heavy run is visited as its part inside [a, b) (piece = true).
-template <typename F>
+template <int R, int NT, typename F>
 __device__ __forceinline__ void for_runs(const uint16_t* sslot, const uint32_t* cur, int a, int b, int L, F fn)
 {
   int p = a;
   if (p < b) {
-    const int s = sslot[p];
+    const int s = sslot[stage_at<R, NT>(p)];
     const int rs = (int)cur[s], re = (int)cur[s + 1];
     if (rs < a) {
       if (re - rs > L) {
@@ -297,7 +307,7 @@ __device__ __forceinline__ void for_runs(const uint16_t* sslot, const uint32_t* 
     }
   }
   while (p < b) {
-    const int s = sslot[p];
+    const int s = sslot[stage_at<R, NT>(p)];
     const int re = (int)cur[s + 1];
     if (re - p <= L) {
       fn(p, re - p, s, false);
@@ -311,7 +321,7 @@ __device__ __forceinline__ void for_runs(const uint16_t* sslot, const uint32_t* 
 }
 
 // P4 for one value column of type (CAT, W).
-template <int CAT, int W>
+template <int CAT, int W, int R, int NT>
 __device__ __forceinline__ void sorted_column(const ValCol& c, int v, uint8_t* table, uint32_t tbase, int stride,
                                               const uint16_t* sslot, const uint8_t* sbits, const uint8_t* stage,
                                               const uint32_t* cur, int a, int b, int L)
@@ -326,13 +336,14 @@ __device__ __forceinline__ void sorted_column(const ValCol& c, int v, uint8_t* t
   uint64_t tsum = 0, tsq = 0, tmn = 0, tmx = 0;
   uint32_t tn = 0, tnull = 0;
   int tslot = -1;
-  for_runs(sslot, cur, a, b, L, [&](int pos, int len, int s, bool piece) {
+  for_runs<R, NT>(sslot, cur, a, b, L, [&](int pos, int len, int s, bool piece) {
     Acc acc;
     acc.init();
     uint32_t nulls = 0;
     for (int p = pos; p < pos + len; ++p) {
-      const bool valid = sbits == nullptr || ((sbits[p] >> v) & 1);
-      const uint64_t x = SW == 8 ? ((const uint64_t*)stage)[p] : ((const uint32_t*)stage)[p];
+      const int q = stage_at<R, NT>(p);
+      const bool valid = sbits == nullptr || ((sbits[q] >> v) & 1);
+      const uint64_t x = SW == 8 ? ((const uint64_t*)stage)[q] : ((const uint32_t*)stage)[q];
       if (valid) acc.add(x);
       else ++nulls;
     }
@@ -404,6 +415,7 @@ __global__ void __launch_bounds__(NT, 1) k_part_sorted(const __grid_constant__ P
                                                        const __grid_constant__ SlotTemplate tmpl)
 {
   static_assert(R % 2 == 0, "rows are loaded in pairs");
+  static_assert((R & (R - 1)) == 0, "rows per thread: a power of two (stage_at)");
   constexpr int C = R * NT;
   constexpr int64_t STEP = C;
   extern __shared__ __align__(16) uint8_t smem[];
@@ -576,7 +588,7 @@ __global__ void __launch_bounds__(NT, 1) k_part_sorted(const __grid_constant__ P
 #pragma unroll
       for (int j = 0; j < R; ++j) {
         if (slot[j] < 0) continue;
-        const uint32_t pos = cur[slot[j]] + rank[j];
+        const int pos = stage_at<R, NT>((int)(cur[slot[j]] + rank[j]));
         sslot[pos] = (uint16_t)slot[j];
         if (have_bits) sbits[pos] = (uint8_t)cvb[j];
         uint8_t* st = stage0;
@@ -595,7 +607,7 @@ __global__ void __launch_bounds__(NT, 1) k_part_sorted(const __grid_constant__ P
       __syncthreads();
       // P4: rows per slot, then every column, run by run
       const int a = threadIdx.x * R, b = min(a + R, (int)s_total);
-      for_runs(sslot, cur, a, b, L, [&](int pos, int len, int s, bool piece) {
+      for_runs<R, NT>(sslot, cur, a, b, L, [&](int pos, int len, int s, bool piece) {
         (void)pos;
         if (!piece) *(uint32_t*)(smem + (size_t)s * stride + P2.rows_off) += (uint32_t)len;
         else sred_add_u32(tbase + (uint32_t)s * (uint32_t)stride + P2.rows_off, (uint32_t)len);
@@ -607,7 +619,7 @@ __global__ void __launch_bounds__(NT, 1) k_part_sorted(const __grid_constant__ P
           if (v >= nv) break;
           const ValCol& c = P2.vals[v];
 #define GB_SORTED_COL(CAT_, W_) \
-  sorted_column<CAT_, W_>(c, v, smem, tbase, stride, sslot, sbits, st, cur, a, b, L)
+  sorted_column<CAT_, W_, R, NT>(c, v, smem, tbase, stride, sslot, sbits, st, cur, a, b, L)
           switch ((c.cat << 4) | c.width) {
             case (CAT_F64 << 4) | 8: GB_SORTED_COL(CAT_F64, 8); break;
             case (CAT_F32 << 4) | 4: GB_SORTED_COL(CAT_F32, 4); break;
