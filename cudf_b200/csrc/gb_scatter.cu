@@ -7,39 +7,52 @@
 namespace gb {
 
 namespace {
-constexpr int kBulkThreads = 512;
-constexpr int kBulkRows = 2048;
-
-template <int KW>
-const void* bulk_kernel()
-{
-  return (const void*)k_part_scatter_bulk<KW, kBulkThreads, kBulkRows>;
-}
+// Launch shapes: 4096-row tiles with one 1024-thread CTA per SM where the
+// tile's layout fits shared memory, else 2048-row tiles with two 512-thread
+// CTAs per SM.
+constexpr int kBigRows = 4096, kBigThreads = 1024;
+constexpr int kRows = 2048, kThreads = 512;
 }  // namespace
 
 size_t part_scatter_bulk_plan(const Plan& P, int nparts, int smem_optin, void* spec_out)
 {
   StageSpec& S = *(StageSpec*)spec_out;
-  if (!part_scatter_bulk_ok(P, kBulkRows, S)) return 0;
-  const size_t sm = part_scatter_bulk_smem(S, P.key_words, kBulkRows, nparts);
-  // static shared memory of the kernel (barrier, scan temporaries) plus slack
-  if (sm + 4096 > (size_t)smem_optin) return 0;
-  return sm;
+  // static shared memory of the kernel (barriers, scan temporaries) plus slack
+  const size_t limit = (size_t)smem_optin - 8192;
+  if (part_scatter_bulk_ok(P, kBigRows, S)) {
+    const size_t sm = part_scatter_bulk_smem(S, P.key_words, kBigRows, nparts);
+    if (sm <= limit) return sm;
+  }
+  if (!part_scatter_bulk_ok(P, kRows, S)) return 0;
+  const size_t sm = part_scatter_bulk_smem(S, P.key_words, kRows, nparts);
+  return 2 * sm <= limit ? sm : 0;
 }
 
 size_t part_scatter_spec_bytes() { return sizeof(StageSpec); }
 
+namespace {
+template <int KW, int NT, int T, int MINB>
+void launch_bulk(const Plan& P, const PartArgs& A, const StageSpec& S, size_t smem, cudaStream_t stream)
+{
+  const void* k = (const void*)k_part_scatter_bulk<KW, NT, T, MINB>;
+  allow_max_smem(k);
+  const int64_t ntiles = (P.num_rows + T - 1) / T;
+  const int grid = (int)std::min<int64_t>(grid_for(k, NT, smem, MINB), ntiles);
+  k_part_scatter_bulk<KW, NT, T, MINB><<<grid, NT, smem, stream>>>(P, A, S);
+}
+}  // namespace
+
 void launch_part_scatter_bulk(const Plan& P, const PartArgs& A, const void* spec, size_t smem, cudaStream_t stream)
 {
   const StageSpec& S = *(const StageSpec*)spec;
-  const void* k = P.key_words == 1 ? bulk_kernel<1>() : bulk_kernel<2>();
-  allow_max_smem(k);
-  const int64_t ntiles = (P.num_rows + kBulkRows - 1) / kBulkRows;
-  const int grid = (int)std::min<int64_t>(grid_for(k, kBulkThreads, smem, 2), ntiles);
-  if (P.key_words == 1)
-    k_part_scatter_bulk<1, kBulkThreads, kBulkRows><<<grid, kBulkThreads, smem, stream>>>(P, A, S);
-  else
-    k_part_scatter_bulk<2, kBulkThreads, kBulkRows><<<grid, kBulkThreads, smem, stream>>>(P, A, S);
+  const bool is_big = S.tile_rows == kBigRows;
+  if (P.key_words == 1) {
+    if (is_big) launch_bulk<1, kBigThreads, kBigRows, 1>(P, A, S, smem, stream);
+    else launch_bulk<1, kThreads, kRows, 2>(P, A, S, smem, stream);
+  } else {
+    if (is_big) launch_bulk<2, kBigThreads, kBigRows, 1>(P, A, S, smem, stream);
+    else launch_bulk<2, kThreads, kRows, 2>(P, A, S, smem, stream);
+  }
 }
 
 }  // namespace gb

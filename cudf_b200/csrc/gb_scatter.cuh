@@ -14,10 +14,14 @@
 //   D  write every output array of the tile in sorted order: consecutive
 //      threads write consecutive rows of a run, the values gathered from the
 //      staged columns, so no column needs a barrier of its own.
-// Two CTAs share an SM: while one works through a tile, the other's copies are
-// in flight.  Tiles are 16-byte aligned only when every staged column starts
-// on a suitable row (see part_scatter_bulk_ok); the last, partial tile is
-// staged with plain loads.
+// The staged arrays form two groups, each completing on its own mbarrier: the
+// key group (key columns and their masks, read only by A) and the value group
+// (value columns and their masks, read only by D).  The next tile's key group
+// is copied in as soon as A is done with this tile's, so it lands during B-D;
+// the next tile's value group as soon as D is done, so it lands during the
+// next tile's A-C.  Tiles are 16-byte aligned only when every staged column
+// starts on a suitable row (see part_scatter_bulk_ok); the last, partial tile
+// is staged with plain loads.
 //
 // Waits on the mbarrier are bounded: a copy that has not landed after the
 // limit sets counters[14] (the host reports a CUDA error) and the CTA stops
@@ -45,8 +49,10 @@ struct StageSpec {
   const uint8_t* src[kMaxStaged];
   int32_t width[kMaxStaged];      // bytes per row; 0 for a mask
   int32_t soff[kMaxStaged];       // byte offset in shared memory
+  int32_t group[kMaxStaged];      // 0: read by the key phase (keys, key masks), 1: by the write-out
   int32_t stage_bytes;            // all arrays of one tile, with their alignment
-  int32_t tx_bytes;               // bytes the copies of a full tile deliver
+  int32_t tx_bytes[2];            // bytes a full tile's copies of each group deliver
+  int32_t tile_rows;              // rows per tile the layout was made for
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -145,15 +151,15 @@ inline size_t part_scatter_bulk_smem(const StageSpec& S, int kw, int T, int npar
   return b;
 }
 
-template <int KW, int NT, int T>
-__global__ void __launch_bounds__(NT, 2) k_part_scatter_bulk(const __grid_constant__ Plan P,
+template <int KW, int NT, int T, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_part_scatter_bulk(const __grid_constant__ Plan P,
                                                              const __grid_constant__ PartArgs A,
                                                              const __grid_constant__ StageSpec S)
 {
   static_assert(T % 128 == 0 && T % NT == 0 && T <= 65536, "tile rows");
   constexpr int RPT = T / NT;
   extern __shared__ __align__(128) uint8_t sm[];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bar[2];
   __shared__ unsigned int s_valid, s_stop;
   using Scan = cub::BlockScan<unsigned, NT>;
   __shared__ typename Scan::TempStorage scan_tmp;
@@ -177,57 +183,74 @@ __global__ void __launch_bounds__(NT, 2) k_part_scatter_bulk(const __grid_consta
   const int per = (A.nparts + NT - 1) / NT;
   constexpr int kWaitLimit = 1 << 22;
   if (threadIdx.x == 0) {
-    mbar_init(&bar, 1);
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_stop = 0;
   }
   __syncthreads();
-  // one thread issues a full tile's copies
-  auto issue = [&](int64_t t0) {
-    mbar_expect_tx(&bar, (unsigned)S.tx_bytes);
+  // one thread issues the copies of a full tile's group g
+  auto issue = [&](int g, int64_t t0) {
+    mbar_expect_tx(&bar[g], (unsigned)S.tx_bytes[g]);
 #pragma unroll 1
     for (int a = 0; a < S.narr; ++a) {
+      if (S.group[a] != g) continue;
       const int w = S.width[a];
       const uint8_t* src = w ? S.src[a] + t0 * w : S.src[a] + (t0 >> 3);
-      bulk_g2s(sm + S.soff[a], src, w ? (unsigned)(T * w) : (unsigned)(T / 8), &bar);
+      bulk_g2s(sm + S.soff[a], src, w ? (unsigned)(T * w) : (unsigned)(T / 8), &bar[g]);
     }
   };
-  unsigned phase = 0;
+  // plain loads of group g of a partial tile into the same layout
+  auto plain = [&](int g, int64_t t0, int cnt) {
+#pragma unroll 1
+    for (int a = 0; a < S.narr; ++a) {
+      if (S.group[a] != g) continue;
+      const int w = S.width[a];
+      uint8_t* d = sm + S.soff[a];
+      if (w) {
+        for (int i = threadIdx.x; i < cnt; i += NT) {
+          const uint8_t* s = S.src[a] + (t0 + i) * w;
+          switch (w) {
+            case 1: d[i] = __ldg(s); break;
+            case 2: ((uint16_t*)d)[i] = __ldg((const uint16_t*)s); break;
+            case 4: ((uint32_t*)d)[i] = __ldg((const uint32_t*)s); break;
+            default: ((uint64_t*)d)[i] = __ldg((const unsigned long long*)s); break;
+          }
+        }
+      } else {
+        const uint32_t* s = (const uint32_t*)(S.src[a] + (t0 >> 3));
+        for (int i = threadIdx.x; i < (cnt + 31) / 32; i += NT) ((uint32_t*)d)[i] = __ldg(s + i);
+      }
+    }
+  };
+  unsigned phase[2] = {0, 0};
+  bool pending[2] = {false, false};  // thread 0's view: copies issued, not yet waited for
+  auto wait_group = [&](int g) {
+    if (mbar_wait(&bar[g], phase[g], kWaitLimit)) {
+      phase[g] ^= 1;
+      pending[g] = false;
+    } else {  // still in flight: reported, and waited for again before exit
+      atomicOr(A.counters + 14, 1u);
+      s_stop = 1;
+    }
+  };
   int64_t tile = blockIdx.x;
-  if (threadIdx.x == 0 && tile < ntiles && (tile + 1) * T <= n) issue(tile * T);
+  if (threadIdx.x == 0 && tile < ntiles && (tile + 1) * T <= n) {
+    issue(0, tile * T);
+    issue(1, tile * T);
+  }
+  pending[0] = pending[1] = tile < ntiles && (tile + 1) * T <= n;
   for (; tile < ntiles; tile += gridDim.x) {
     const int64_t t0 = tile * T;
     const int cnt = (int)min((int64_t)T, n - t0);
+    const int64_t nt = tile + gridDim.x;
+    const bool next_full = nt < ntiles && (nt + 1) * T <= n;
     for (int i = threadIdx.x; i < A.nparts; i += NT) hist[i] = 0;
     if (cnt == T) {
-      // a full tile: its copies were issued at the end of the previous one
-      const bool ok = mbar_wait(&bar, phase, kWaitLimit);
-      phase ^= 1;
-      if (!ok) {
-        atomicOr(A.counters + 14, 1u);
-        s_stop = 1;
-      }
+      wait_group(0);  // issued one tile earlier, after A
     } else {
-      // the partial last tile: plain loads into the same layout
-#pragma unroll 1
-      for (int a = 0; a < S.narr; ++a) {
-        const int w = S.width[a];
-        uint8_t* d = sm + S.soff[a];
-        if (w) {
-          for (int i = threadIdx.x; i < cnt; i += NT) {
-            const uint8_t* s = S.src[a] + (t0 + i) * w;
-            switch (w) {
-              case 1: d[i] = __ldg(s); break;
-              case 2: ((uint16_t*)d)[i] = __ldg((const uint16_t*)s); break;
-              case 4: ((uint32_t*)d)[i] = __ldg((const uint32_t*)s); break;
-              default: ((uint64_t*)d)[i] = __ldg((const unsigned long long*)s); break;
-            }
-          }
-        } else {
-          const uint32_t* s = (const uint32_t*)(S.src[a] + (t0 >> 3));
-          for (int i = threadIdx.x; i < (cnt + 31) / 32; i += NT) ((uint32_t*)d)[i] = __ldg(s + i);
-        }
-      }
+      plain(0, t0, cnt);
+      plain(1, t0, cnt);
     }
     __syncthreads();
     if (s_stop) break;
@@ -247,6 +270,14 @@ __global__ void __launch_bounds__(NT, 2) k_part_scatter_bulk(const __grid_consta
       if (KW == 2) kw1[k] = w1;
     }
     __syncthreads();
+    // the key group is free: the next full tile's keys land during B-D
+    if (next_full) {
+      if (threadIdx.x == 0) {
+        fence_async_shared();
+        issue(0, nt * T);
+      }
+      pending[0] = true;
+    }
     // B: reservations, then the scan (as k_part_scatter)
     unsigned mine = 0;
     for (int q0 = threadIdx.x * per; q0 < min(A.nparts, (threadIdx.x + 1) * per); q0 += 4) {
@@ -294,7 +325,9 @@ __global__ void __launch_bounds__(NT, 2) k_part_scatter_bulk(const __grid_consta
       kst[KW * s] = kw0[k];
       if (KW == 2) kst[2 * s + 1] = kw1[k];
     }
+    if (cnt == T) wait_group(1);  // issued after the previous tile's write-out
     __syncthreads();
+    if (s_stop) break;
     // D: every output array in sorted order
     const int nvalid = (int)s_valid;
     for (int s = threadIdx.x; s < nvalid; s += NT) {
@@ -320,16 +353,20 @@ __global__ void __launch_bounds__(NT, 2) k_part_scatter_bulk(const __grid_consta
       if (any_bits) A.bits[g] = (uint8_t)vb;
     }
     __syncthreads();
-    // the next full tile's copies into the now free stage
-    const int64_t nt = tile + gridDim.x;
-    if (threadIdx.x == 0 && nt < ntiles && (nt + 1) * T <= n) {
-      fence_async_shared();
-      issue(nt * T);
+    // the value group is free: the next full tile's values land during its A-C
+    if (next_full) {
+      if (threadIdx.x == 0) {
+        fence_async_shared();
+        issue(1, nt * T);
+      }
+      pending[1] = true;
     }
   }
   // leave no copy in flight: a CTA that stopped early waits (bounded) for
-  // the phase it was waiting on
-  if (s_stop && threadIdx.x == 0) mbar_wait(&bar, phase ^ 1, kWaitLimit);
+  // the groups it had issued
+  if (s_stop && threadIdx.x == 0)
+    for (int g = 0; g < 2; ++g)
+      if (pending[g]) mbar_wait(&bar[g], phase[g], kWaitLimit);
 }
 
 // Whether every array the plan reads can be bulk-copied tile by tile: data
@@ -341,7 +378,8 @@ inline bool part_scatter_bulk_ok(const Plan& P, int T, StageSpec& S)
   std::memset(&S, 0, sizeof(S));
   if (P.num_vals > 8 || P.num_keys > kMaxKeyCols) return false;
   int a = 0;
-  size_t off = 0, tx = 0;
+  size_t off = 0, tx[2] = {0, 0};
+  int grp = 0;
   auto add = [&](const void* data, int64_t offset, int width) -> int {
     if (a >= kMaxStaged) return -2;
     const uint8_t* src;
@@ -356,9 +394,10 @@ inline bool part_scatter_bulk_ok(const Plan& P, int T, StageSpec& S)
     S.src[a] = src;
     S.width[a] = width;
     S.soff[a] = (int32_t)off;
+    S.group[a] = grp;
     const size_t bytes = width ? (size_t)T * width : (size_t)T / 8;
     off = (off + bytes + 15) & ~(size_t)15;
-    tx += bytes;
+    tx[grp] += bytes;
     return a++;
   };
   for (int k = 0; k < P.num_keys; ++k) {
@@ -368,6 +407,7 @@ inline bool part_scatter_bulk_ok(const Plan& P, int T, StageSpec& S)
     S.key_mask[k] = c.mask ? add(c.mask, c.offset, 0) : -1;
     if (S.key_data[k] == -2 || S.key_mask[k] == -2) return false;
   }
+  grp = 1;
   for (int v = 0; v < P.num_vals; ++v) {
     const ValCol& c = P.vals[v];
     if (c.width != 1 && c.width != 2 && c.width != 4 && c.width != 8) return false;
@@ -377,7 +417,9 @@ inline bool part_scatter_bulk_ok(const Plan& P, int T, StageSpec& S)
   }
   S.narr = a;
   S.stage_bytes = (int32_t)off;
-  S.tx_bytes = (int32_t)tx;
+  S.tx_bytes[0] = (int32_t)tx[0];
+  S.tx_bytes[1] = (int32_t)tx[1];
+  S.tile_rows = T;
   return true;
 }
 
