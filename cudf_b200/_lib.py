@@ -45,7 +45,8 @@ class GbTuning(ctypes.Structure):
                 ("smem_bytes", ctypes.c_int32), ("smem_fill_pct", ctypes.c_int32),
                 ("smem_max_groups", ctypes.c_int64), ("load_factor_pct", ctypes.c_int32),
                 ("force_mode", ctypes.c_int32), ("groups_hint", ctypes.c_int64),
-                ("profile", ctypes.c_int32), ("scatter", ctypes.c_int32), ("pass2", ctypes.c_int32)]
+                ("profile", ctypes.c_int32), ("scatter", ctypes.c_int32), ("pass2", ctypes.c_int32),
+                ("part_fill_pct", ctypes.c_int32)]
 
 
 class GbStats(ctypes.Structure):

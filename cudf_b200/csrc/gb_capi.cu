@@ -178,6 +178,11 @@ static uint32_t apply_tuning(const gb_tuning* t, gb::Options& o)
     o.scatter = t->scatter;
     m |= gb::OPT_SCATTER;
   }
+  if (t->part_fill_pct > 0) {
+    if (t->part_fill_pct > 95) throw gb::Error(gb::ERR_LOGIC, "part_fill_pct must be in [1, 95]");
+    o.part_fill = t->part_fill_pct / 100.0;
+    m |= gb::OPT_PART_FILL;
+  }
   if (t->pass2 >= 0) {
     if (t->pass2 > 3) throw gb::Error(gb::ERR_LOGIC, "pass2 must be in [0, 3]");
     o.pass2 = t->pass2;

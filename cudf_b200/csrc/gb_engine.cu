@@ -545,6 +545,7 @@ int apply_tuning_rules(Options& o, int64_t rows, int64_t groups, int key_words)
     if (m & OPT_MODE) o.force_mode = r.opt.force_mode;
     if (m & OPT_SCATTER) o.scatter = r.opt.scatter;
     if (m & OPT_PASS2) o.pass2 = r.opt.pass2;
+    if (m & OPT_PART_FILL) o.part_fill = r.opt.part_fill;
     return (int)i;
   }
   return -1;
@@ -694,7 +695,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   constexpr int kMaxParts = 8192;
   int nparts = 0;
   if (part_ok) {
-    double per = scap2 * 0.7;
+    double per = scap2 * opt.part_fill;
     nparts = (int)std::min<uint64_t>(kMaxParts, std::max<uint64_t>(2, next_pow2((uint64_t)std::ceil(est / per))));
   }
   const bool part_fits = (double)est <= 0.85 * (double)kMaxParts * sfill2;

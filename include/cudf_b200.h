@@ -140,14 +140,17 @@ typedef struct gb_tuning {
   int32_t force_mode;
   int64_t groups_hint;      /* caller's estimate of the number of groups (skips sampling) */
   int32_t profile;          /* 1: time the aggregation and compaction kernels with CUDA events */
-  int32_t scatter;          /* partitioned pass 1: 0-6 the per-thread launch shapes, threads x rows
-                               per thread: 0 512x8 (default), 1 256x16, 2 512x16, 3 1024x8, 4 512x8
-                               with the next column's loads issued early, 5 1024x4, 6 256x8;
-                               7 tiles of 2048 rows staged in shared memory by bulk copies when
-                               every column allows it (16-byte aligned rows), else 0 */
+  int32_t scatter;          /* partitioned pass 1: 7 (default) tiles of 4096 (or 2048) rows staged in
+                               shared memory by bulk copies when every column allows it (16-byte
+                               aligned rows), else 0; 0-6 the per-thread launch shapes, threads x
+                               rows per thread: 0 512x8, 1 256x16, 2 512x16, 3 1024x8, 4 512x8 with
+                               the next column's loads issued early, 5 1024x4, 6 256x8 */
   int32_t pass2;            /* partitioned pass 2: 1 per-row shared reductions (default); 0 (or 2)
                                chunks counting-sorted by slot, 512 threads x 4 rows; 3 sorted,
                                256 threads x 8 rows */
+  int32_t part_fill_pct;    /* partitioned mode: expected groups per partition as a percentage of
+                               the pass-2 shared table's slots (default 70; sets the partition
+                               count, a power of two) */
 } gb_tuning;
 
 /* What the last gb_aggregate on a handle did. */
