@@ -936,6 +936,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
       ck(cudaGetLastError(), "partition aggregate launch");
       if (deferred) {
         // counts and flags stay on the device until the compaction is done
+        mark("partition passes launched");
         done = true;
         dense_n = -1;
         cap = spill_cap;
@@ -1078,6 +1079,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   }
   st.capacity = (int64_t)cap;
   mark("aggregate done");
+  mark("outputs");
   // deferred: outputs are sized for every slot that could hold a group
   int64_t G_n = deferred ? -1 : (int64_t)host[0] + dense_n;
   const int64_t out_rows = deferred ? (dense ? dense_cap : 0) + (int64_t)cap + 1 : G_n;
