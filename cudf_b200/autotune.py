@@ -183,13 +183,7 @@ def tune_batch(instances: int = 512, steps: int = 3, verbose: bool = False) -> T
     del mix
     rules = []
     for r_hi, g_hi in BATCH_BUCKETS:
-        lo_r = 4097 if r_hi == 16384 else r_hi // 16
-        sizes = []
-        for _ in range(32 if r_hi <= 262144 else 8):
-            n = int(np.exp(rng.uniform(np.log(lo_r), np.log(r_hi))))
-            g = int(min(n, np.exp(rng.uniform(np.log(max(2, g_hi // 16)), np.log(min(g_hi, 1 << 20))))))
-            sizes.append((n, max(2, g)))
-        inst = _batch_workload(sizes, r_hi ^ g_hi)
+        inst = _batch_workload(bucket_sizes(rng, r_hi, g_hi), r_hi ^ g_hi)
         cand_best, cand_ms = None, None
         for cand in [{}] + _BATCH_RULE_CANDS:
             rule = {"max_rows": r_hi, "max_groups": g_hi, **cand}
@@ -207,6 +201,24 @@ def tune_batch(instances: int = 512, steps: int = 3, verbose: bool = False) -> T
     if verbose:
         print(f"batch launch: {best} {best_ms:.3f} ms", flush=True)
     return {"launch": best, "rules": rules}, {"launch_ms": best_ms, "trials": log}
+
+
+def bucket_sizes(rng, r_hi: int, g_hi: int) -> List[Tuple[int, int]]:
+    """(rows, groups) of the instances a bucket is tuned on: rows
+    log-uniform over the top sixteenth of the bucket's row range (from 4097
+    for the smallest), groups log-uniform over the top sixteenth of its group
+    range, the open-ended bucket from 65536 to 2^20; never more groups than
+    rows."""
+    import numpy as np
+    lo_r = 4097 if r_hi == 16384 else r_hi // 16
+    hi_g = min(g_hi, 1 << 20)
+    lo_g = max(2, min(g_hi // 16, 65536))
+    sizes = []
+    for _ in range(32 if r_hi <= 262144 else 8):
+        n = int(np.exp(rng.uniform(np.log(lo_r), np.log(r_hi))))
+        g = int(min(n, np.exp(rng.uniform(np.log(lo_g), np.log(hi_g)))))
+        sizes.append((n, max(2, g)))
+    return sizes
 
 
 def order_rules(rules: Sequence[Dict]) -> List[Dict]:

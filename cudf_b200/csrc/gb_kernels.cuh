@@ -272,6 +272,26 @@ __device__ __forceinline__ void count_nulls(bool is_null, unsigned int* counter)
   if (m && (threadIdx.x & 31) == (__ffs(m) - 1)) atomicAdd(counter, __popc(m));
 }
 
+// Sets the validity bits of a warp's output rows.  The occupied lanes of a
+// warp write consecutive positions (pos of the lowest occupied lane, + 1 per
+// occupied lane), so their bits form one run: assembled with one warp OR
+// reduction and stored with at most two atomic ORs instead of one per row.
+// Every lane of the warp calls it.
+__device__ __forceinline__ void warp_mask_or(uint32_t* mask, bool occ, bool bit, int64_t pos)
+{
+  const unsigned full = 0xFFFFFFFFu;
+  const unsigned occm = __ballot_sync(full, occ);
+  if (!occm) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned rank = __popc(occm & ((1u << lane) - 1));
+  const unsigned word = __reduce_or_sync(full, (occ && bit) ? (1u << rank) : 0u);
+  if (lane == __ffs(occm) - 1 && word) {
+    const int sh = (int)(pos & 31);
+    atomicOr(mask + (pos >> 5), word << sh);
+    if (sh && (word >> (32 - sh))) atomicOr(mask + (pos >> 5) + 1, word >> (32 - sh));
+  }
+}
+
 // Value bits of output j for a slot, and whether it is valid.
 __device__ __forceinline__ uint64_t finalize(const Plan& P, const OutSpec& o, const uint8_t* slot,
                                              bool& valid)
@@ -349,35 +369,32 @@ __device__ __forceinline__ void compact_block(const Plan& P, const uint8_t* T, i
     atomicOr(O.counters + 1, 1u);  // more occupied slots than counted groups
     occ = false;
   }
+  // every lane of the block runs what follows (warp-wide mask assembly)
+  const int64_t pos = (int64_t)*s_base + local;
+  uint64_t w[2] = {0, 0};
   if (occ) {
-    int64_t pos = (int64_t)*s_base + local;
-    uint64_t w[2] = {((const uint64_t*)slot)[0], P.key_words == 2 ? ((const uint64_t*)slot)[1] : 0};
-    for (int k = 0; k < P.num_keys; ++k) {
-      const KeyCol& c = P.keys[k];
-      bool is_null = c.has_null_bit && ((w[c.null_word] >> c.null_shift) & 1);
-      uint64_t bits = c.width == 8 ? w[c.word] : (w[c.word] >> c.shift) & ((1ull << (8 * c.width)) - 1);
-      store_width(O.key_data[k], pos, c.width, is_null ? 0 : bits);
-      if (O.key_mask[k] && !is_null) atomicOr(O.key_mask[k] + (pos >> 5), 1u << (pos & 31));
-    }
-    for (int j = 0; j < P.num_outs; ++j) {
-      const OutSpec& o = P.outs[j];
-      bool valid;
-      uint64_t bits = finalize(P, o, slot, valid);
-      store_width(O.out_data[j], pos, o.out_width, valid ? bits : 0);
-      if (O.out_mask[j] && valid) atomicOr(O.out_mask[j] + (pos >> 5), 1u << (pos & 31));
-    }
+    w[0] = ((const uint64_t*)slot)[0];
+    w[1] = P.key_words == 2 ? ((const uint64_t*)slot)[1] : 0;
   }
-  // null counts (warp-aggregated)
   for (int k = 0; k < P.num_keys; ++k) {
     const KeyCol& c = P.keys[k];
-    bool is_null = occ && c.has_null_bit &&
-                   (((P.key_words == 2 && c.null_word == 1 ? ((const uint64_t*)slot)[1] : ((const uint64_t*)slot)[0])
-                     >> c.null_shift) & 1);
+    const bool is_null = occ && c.has_null_bit && ((w[c.null_word] >> c.null_shift) & 1);
+    if (occ) {
+      const uint64_t bits = c.width == 8 ? w[c.word] : (w[c.word] >> c.shift) & ((1ull << (8 * c.width)) - 1);
+      store_width(O.key_data[k], pos, c.width, is_null ? 0 : bits);
+    }
+    if (O.key_mask[k]) warp_mask_or(O.key_mask[k], occ, !is_null, pos);
     count_nulls(is_null, O.counters + 4 + k);
   }
   for (int j = 0; j < P.num_outs; ++j) {
+    const OutSpec& o = P.outs[j];
     bool valid = true;
-    if (occ && P.outs[j].nullable) finalize(P, P.outs[j], slot, valid);
+    uint64_t bits = 0;
+    if (occ) {
+      bits = finalize(P, o, slot, valid);
+      store_width(O.out_data[j], pos, o.out_width, valid ? bits : 0);
+    }
+    if (O.out_mask[j]) warp_mask_or(O.out_mask[j], occ, valid, pos);
     count_nulls(occ && !valid, O.counters + 4 + P.num_keys + j);
   }
   __syncthreads();

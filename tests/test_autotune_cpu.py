@@ -42,3 +42,17 @@ def test_batch_tuning_install_and_reject():
     with pytest.raises(ValueError):
         autotune.set_batch_tuning([], {"block": 512, "tile_rows": 10, "smem_bytes": 0})
     autotune.set_batch_tuning([], autotune.BATCH_LAUNCH_DEFAULT)
+
+
+def test_batch_bucket_sizes_stay_inside_their_bucket():
+    import numpy as np
+    rng = np.random.default_rng(0)
+    bounds = sorted({g for _, g in autotune.BATCH_BUCKETS})
+    for r_hi, g_hi in autotune.BATCH_BUCKETS:
+        sizes = autotune.bucket_sizes(rng, r_hi, g_hi)
+        assert sizes
+        g_lo = max([b for b in bounds if b < g_hi], default=1)
+        for n, g in sizes:
+            assert 1 <= n <= r_hi and 2 <= g <= n
+            # groups from the bucket's own range unless the rows cap them
+            assert g <= g_hi and (g > g_lo // 16 or g == max(2, n))
