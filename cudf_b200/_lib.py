@@ -46,7 +46,7 @@ class GbTuning(ctypes.Structure):
                 ("smem_max_groups", ctypes.c_int64), ("load_factor_pct", ctypes.c_int32),
                 ("force_mode", ctypes.c_int32), ("groups_hint", ctypes.c_int64),
                 ("profile", ctypes.c_int32), ("scatter", ctypes.c_int32), ("pass2", ctypes.c_int32),
-                ("part_fill_pct", ctypes.c_int32)]
+                ("part_fill_pct", ctypes.c_int32), ("wagg_pct", ctypes.c_int32)]
 
 
 class GbStats(ctypes.Structure):

@@ -36,7 +36,7 @@ TUNING_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning_b
 # fields of a rule's tuning, with the value meaning "unset" in gb_tuning
 _UNSET = {"block": -1, "blocks_per_sm": -1, "smem_bytes": -1, "smem_fill_pct": -1, "smem_max_groups": -1,
           "load_factor_pct": -1, "force_mode": -2, "groups_hint": -1, "profile": -1, "scatter": -1,
-          "pass2": -1, "part_fill_pct": -1}
+          "pass2": -1, "part_fill_pct": -1, "wagg_pct": -1}
 
 # default buckets: row counts x group counts seen by the benchmark shapes
 DEFAULT_BUCKETS = [
@@ -48,7 +48,7 @@ DEFAULT_BUCKETS = [
 
 # candidate settings per stage of the search (coordinate descent)
 _MODES = [{"force_mode": -1}, {"force_mode": 0}, {"force_mode": 1}, {"force_mode": 2}]
-_SCATTER = [{"scatter": s} for s in range(8)]
+_SCATTER = [{"scatter": s} for s in range(9)]
 _SMEM = [{"smem_bytes": b, "smem_fill_pct": f} for b in (48 << 10, 96 << 10, 160 << 10) for f in (50, 70)]
 _LOAD = [{"load_factor_pct": p} for p in (40, 50, 70)]
 

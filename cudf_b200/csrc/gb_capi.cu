@@ -174,7 +174,7 @@ static uint32_t apply_tuning(const gb_tuning* t, gb::Options& o)
   if (t->groups_hint >= 0) o.groups_hint = t->groups_hint;
   if (t->profile >= 0) o.profile = t->profile;
   if (t->scatter >= 0) {
-    if (t->scatter > 7) throw gb::Error(gb::ERR_LOGIC, "scatter must be in [0, 7]");
+    if (t->scatter > 8) throw gb::Error(gb::ERR_LOGIC, "scatter must be in [0, 8]");
     o.scatter = t->scatter;
     m |= gb::OPT_SCATTER;
   }
@@ -183,8 +183,9 @@ static uint32_t apply_tuning(const gb_tuning* t, gb::Options& o)
     o.part_fill = t->part_fill_pct / 100.0;
     m |= gb::OPT_PART_FILL;
   }
+  if (t->wagg_pct >= 0) o.wagg_pct = t->wagg_pct, m |= gb::OPT_WAGG;
   if (t->pass2 >= 0) {
-    if (t->pass2 > 3) throw gb::Error(gb::ERR_LOGIC, "pass2 must be in [0, 3]");
+    if (t->pass2 > 4) throw gb::Error(gb::ERR_LOGIC, "pass2 must be in [0, 4]");
     o.pass2 = t->pass2;
     m |= gb::OPT_PASS2;
   }

@@ -546,6 +546,7 @@ int apply_tuning_rules(Options& o, int64_t rows, int64_t groups, int key_words)
     if (m & OPT_SCATTER) o.scatter = r.opt.scatter;
     if (m & OPT_PASS2) o.pass2 = r.opt.pass2;
     if (m & OPT_PART_FILL) o.part_fill = r.opt.part_fill;
+    if (m & OPT_WAGG) o.wagg_pct = r.opt.wagg_pct;
     return (int)i;
   }
   return -1;
@@ -668,7 +669,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   // that fit beside the chunk's sorted stage and the two per-slot count arrays.
   bool any_val_null = false;
   for (int v = 0; v < P.num_vals; ++v) any_val_null |= P.vals[v].mask != nullptr;
-  const bool p2_sorted = opt.pass2 != 1;
+  const bool p2_sorted = opt.pass2 != 1 && opt.pass2 != 4;
   const int p2_rows = part_sorted_rows(opt.pass2, P.num_vals);  // rows per sorted chunk
   int scap2;
   if (p2_sorted) {
@@ -799,9 +800,12 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
         kern<<<grid, nt, psmem, stream>>>(P, A);
       };
       const bool kw1 = P.key_words == 1;
-      // 7 (the default): tiles staged by bulk copies when every column allows it
+      // 7 (the default): tiles staged by bulk copies when every column allows
+      // it; 8: the same with 2048-row tiles, two CTAs per SM
       std::vector<uint8_t> spec(part_scatter_spec_bytes());
-      const size_t bsm = opt.scatter == 7 ? part_scatter_bulk_plan(P, nparts, dev.smem_optin, spec.data()) : 0;
+      const size_t bsm = opt.scatter >= 7
+                           ? part_scatter_bulk_plan(P, nparts, dev.smem_optin, spec.data(), opt.scatter == 8)
+                           : 0;
       if (bsm) launch_part_scatter_bulk(P, A, spec.data(), bsm, stream);
       else switch (opt.scatter) {
         case 1: kw1 ? launch(k_part_scatter<1, 16, 256, 3>, 256, 16) : launch(k_part_scatter<2, 16, 256, 3>, 256, 16); break;
@@ -832,6 +836,7 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     // handled by several CTAs, each merging its table into the global table
     std::vector<PartItem> items;
     int64_t nsplit = 0;
+    int nwagg = 0;  // leading items taken by the warp-combining launch
     {
       int64_t nrows = 0;
       for (auto r : prows) nrows += r;
@@ -848,15 +853,20 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
             items.push_back(PartItem{p, 1, pbase[p] + b, pbase[p] + std::min(r, b + chunk)});
         }
       }
-      for (int p = 0; p < nparts; ++p) {
-        const int64_t r = prows[p];
-        if (!(exact_buckets && r > 2 * chunk)) items.push_back(PartItem{p, 0, pbase[p], pend[p]});
+      // whole partitions with well over the average rows hold heavy keys:
+      // they follow the split items into the warp-combining launch
+      const double heavy = opt.wagg_pct / 100.0 * ((double)nrows / std::max(1, nparts));
+      for (int pass = 0; pass < 2; ++pass) {
+        for (int p = 0; p < nparts; ++p) {
+          const int64_t r = prows[p];
+          if (exact_buckets && r > 2 * chunk) continue;
+          if ((pass == 0) == ((double)r > heavy || opt.wagg_pct == 0)) items.push_back(PartItem{p, 0, pbase[p], pend[p]});
+        }
+        if (pass == 0) nwagg = (int)items.size();
       }
     }
     PartItem* d_items = (PartItem*)S.get(sizeof(PartItem) * items.size());
     ck(cudaMemcpyAsync(d_items, items.data(), sizeof(PartItem) * items.size(), cudaMemcpyHostToDevice, stream), "h2d");
-    int nmerge = 0;
-    while (nmerge < (int)items.size() && items[nmerge].merge) ++nmerge;
     // groups expected to miss their partition's shared table, plus those of
     // split partitions, go to the global spill table
     const double expect_spill = std::max(0.0, (double)est - 0.85 * (double)nparts * sfill2);
@@ -905,25 +915,33 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
         ++st.kernels;
       };
       const bool few = P.num_vals <= 4;
-      const int nrest = (int)items.size() - nmerge;
+      const int nrest = (int)items.size() - nwagg;
       if (p2_sorted) {
-        launch_s(0, nmerge, counters + 8, true);
-        launch_s(nmerge, nrest, counters + 9, false);
+        launch_s(0, nwagg, counters + 8, true);
+        launch_s(nwagg, nrest, counters + 9, false);
+      } else if (opt.pass2 == 4 && few) {  // 512 threads x 2 rows
+        if (P.key_words == 1) {
+          launch2(k_part_aggregate<1, 2, 512, 4, true>, 512, 0, nwagg, counters + 8);
+          launch2(k_part_aggregate<1, 2, 512, 4, false>, 512, nwagg, nrest, counters + 9);
+        } else {
+          launch2(k_part_aggregate<2, 2, 512, 4, true>, 512, 0, nwagg, counters + 8);
+          launch2(k_part_aggregate<2, 2, 512, 4, false>, 512, nwagg, nrest, counters + 9);
+        }
       } else if (P.key_words == 1) {
         if (few) {
-          launch2(k_part_aggregate<1, 1, 1024, 4, true>, 1024, 0, nmerge, counters + 8);
-          launch2(k_part_aggregate<1, 1, 1024, 4, false>, 1024, nmerge, nrest, counters + 9);
+          launch2(k_part_aggregate<1, 1, 1024, 4, true>, 1024, 0, nwagg, counters + 8);
+          launch2(k_part_aggregate<1, 1, 1024, 4, false>, 1024, nwagg, nrest, counters + 9);
         } else {
-          launch2(k_part_aggregate<1, 1, 1024, 8, true>, 1024, 0, nmerge, counters + 8);
-          launch2(k_part_aggregate<1, 1, 1024, 8, false>, 1024, nmerge, nrest, counters + 9);
+          launch2(k_part_aggregate<1, 1, 1024, 8, true>, 1024, 0, nwagg, counters + 8);
+          launch2(k_part_aggregate<1, 1, 1024, 8, false>, 1024, nwagg, nrest, counters + 9);
         }
       } else {
         if (few) {
-          launch2(k_part_aggregate<2, 1, 1024, 4, true>, 1024, 0, nmerge, counters + 8);
-          launch2(k_part_aggregate<2, 1, 1024, 4, false>, 1024, nmerge, nrest, counters + 9);
+          launch2(k_part_aggregate<2, 1, 1024, 4, true>, 1024, 0, nwagg, counters + 8);
+          launch2(k_part_aggregate<2, 1, 1024, 4, false>, 1024, nwagg, nrest, counters + 9);
         } else {
-          launch2(k_part_aggregate<2, 1, 1024, 8, true>, 1024, 0, nmerge, counters + 8);
-          launch2(k_part_aggregate<2, 1, 1024, 8, false>, 1024, nmerge, nrest, counters + 9);
+          launch2(k_part_aggregate<2, 1, 1024, 8, true>, 1024, 0, nwagg, counters + 8);
+          launch2(k_part_aggregate<2, 1, 1024, 8, false>, 1024, nwagg, nrest, counters + 9);
         }
       }
       if (opt.profile) ck(cudaEventRecord(events()[1], stream), "event");

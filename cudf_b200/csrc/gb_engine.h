@@ -80,6 +80,7 @@ struct Options {
   int scatter = 7;             // partitioned pass 1: 7 bulk-copy tiles where the columns allow (else 0), 0-6 launch shapes of the per-thread scatter
   double part_fill = 0.7;      // partitioned mode: expected groups per partition / shared-table slots (sets the partition count)
   int pass2 = 1;               // partitioned pass 2: 1 per-row shared reductions, 0/2 sorted chunks 512x4, 3 sorted 256x8
+  int wagg_pct = 125;          // partitioned pass 2: warp-combined updates for partitions above this % of the average rows
   uint32_t set_mask = 0;       // OPT_* bits of the fields a caller set explicitly
   // internal: 0 reads every outcome (group counts, overflow flags, null
   // counts) back once, after the compaction, sizing the outputs by an upper
@@ -91,7 +92,7 @@ struct Options {
 // Option fields, as bits of Options::set_mask and TuningRule::mask.
 enum OptBits : uint32_t {
   OPT_BLOCK = 1, OPT_BPS = 2, OPT_SMEM = 4, OPT_FILL = 8, OPT_SMEM_MAX = 16, OPT_LOAD = 32,
-  OPT_MODE = 64, OPT_SCATTER = 128, OPT_PASS2 = 256, OPT_PART_FILL = 512
+  OPT_MODE = 64, OPT_SCATTER = 128, OPT_PASS2 = 256, OPT_PART_FILL = 512, OPT_WAGG = 1024
 };
 
 // A process-wide tuning rule: for calls with at most max_rows rows and at most

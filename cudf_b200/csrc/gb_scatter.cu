@@ -14,12 +14,12 @@ constexpr int kBigRows = 4096, kBigThreads = 1024;
 constexpr int kRows = 2048, kThreads = 512;
 }  // namespace
 
-size_t part_scatter_bulk_plan(const Plan& P, int nparts, int smem_optin, void* spec_out)
+size_t part_scatter_bulk_plan(const Plan& P, int nparts, int smem_optin, void* spec_out, bool small_only)
 {
   StageSpec& S = *(StageSpec*)spec_out;
   // static shared memory of the kernel (barriers, scan temporaries) plus slack
   const size_t limit = (size_t)smem_optin - 8192;
-  if (part_scatter_bulk_ok(P, kBigRows, S)) {
+  if (!small_only && part_scatter_bulk_ok(P, kBigRows, S)) {
     const size_t sm = part_scatter_bulk_smem(S, P.key_words, kBigRows, nparts);
     if (sm <= limit) return sm;
   }

@@ -53,6 +53,8 @@ struct StageSpec {
   int32_t stage_bytes;            // all arrays of one tile, with their alignment
   int32_t tx_bytes[2];            // bytes a full tile's copies of each group deliver
   int32_t tile_rows;              // rows per tile the layout was made for
+  int32_t key8;                   // one 8-byte integer key column without a mask:
+                                  // its staged value is the packed key
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -103,6 +105,17 @@ __device__ __forceinline__ uint64_t staged_bits(const uint8_t* a, int w, int row
 __device__ __forceinline__ bool staged_valid(const uint8_t* m, int row)
 {
   return (((const uint32_t*)m)[row >> 5] >> (row & 31)) & 1u;
+}
+
+// Copies the staged elements rows[k] of one column to their destinations
+// dst[g[k]] (g < 0: nothing to write).
+template <typename W, int RPT>
+__device__ __forceinline__ void scatter_col(void* dst, const uint8_t* src, const int64_t (&g)[RPT],
+                                            const int (&rows)[RPT])
+{
+#pragma unroll
+  for (int k = 0; k < RPT; ++k)
+    if (g[k] >= 0) ((W*)dst)[g[k]] = ((const W*)src)[rows[k]];
 }
 
 // Packs the key of staged row `row` (as pack_key does from HBM).
@@ -257,12 +270,13 @@ __global__ void __launch_bounds__(NT, MINB) k_part_scatter_bulk(const __grid_con
     // A: partition and rank of every row (packed keys kept in registers)
     uint32_t pr[RPT];
     uint64_t kw0[RPT], kw1[KW == 2 ? RPT : 1];
+    const uint64_t* k8 = (KW == 1 && S.key8) ? (const uint64_t*)(sm + S.soff[S.key_data[0]]) : nullptr;
 #pragma unroll
     for (int k = 0; k < RPT; ++k) {
       const int i = k * NT + threadIdx.x;
       pr[k] = 0xFFFFFFFFu;
       uint64_t w0 = 0, w1 = 0;
-      if (i < cnt && pack_key_staged(P, S, sm, i, w0, w1)) {
+      if (i < cnt && (k8 ? (w0 = k8[i], true) : pack_key_staged(P, S, sm, i, w0, w1))) {
         const unsigned p = (unsigned)(hash_key(w0, w1, KW) >> A.shift);
         pr[k] = (p << 16) | atomicAdd(&hist[p], 1u);
       }
@@ -328,29 +342,51 @@ __global__ void __launch_bounds__(NT, MINB) k_part_scatter_bulk(const __grid_con
     if (cnt == T) wait_group(1);  // issued after the previous tile's write-out
     __syncthreads();
     if (s_stop) break;
-    // D: every output array in sorted order
+    // D: every output array in sorted order.  Each thread keeps the
+    // destination and the staged row of its sorted positions in registers and
+    // writes the columns one at a time, so the width dispatch is taken once
+    // per column instead of once per row.
     const int nvalid = (int)s_valid;
-    for (int s = threadIdx.x; s < nvalid; s += NT) {
+    int64_t gdst[RPT];
+    int srow[RPT];
+    uint32_t vb[RPT];
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+      const int s = k * NT + threadIdx.x;
+      gdst[k] = -1;
+      srow[k] = 0;
+      vb[k] = 0;
+      if (s >= nvalid) continue;
       const unsigned p = psort[s];
       if ((unsigned)s >= send[p]) continue;
-      const int64_t g = delta[p] + s;
-      const int row = order[s];
-      if (KW == 1) A.keys[g] = kst[s];
-      else *(ulonglong2*)(A.keys + 2 * g) = make_ulonglong2(kst[2 * s], kst[2 * s + 1]);
-      uint32_t vb = 0;
+      gdst[k] = delta[p] + s;
+      srow[k] = order[s];
+      if (KW == 1) A.keys[gdst[k]] = kst[s];
+      else *(ulonglong2*)(A.keys + 2 * gdst[k]) = make_ulonglong2(kst[2 * s], kst[2 * s + 1]);
+    }
 #pragma unroll 1
-      for (int v = 0; v < nv; ++v) {
-        const int w = P.vals[v].width;
-        const uint64_t x = staged_bits(sm + S.soff[S.val_data[v]], w, row);
-        switch (w) {
-          case 1: ((uint8_t*)A.vals[v])[g] = (uint8_t)x; break;
-          case 2: ((uint16_t*)A.vals[v])[g] = (uint16_t)x; break;
-          case 4: ((uint32_t*)A.vals[v])[g] = (uint32_t)x; break;
-          default: ((uint64_t*)A.vals[v])[g] = x; break;
-        }
-        if (S.val_mask[v] < 0 || staged_valid(sm + S.soff[S.val_mask[v]], row)) vb |= 1u << v;
+    for (int v = 0; v < nv; ++v) {
+      const uint8_t* src = sm + S.soff[S.val_data[v]];
+      switch (P.vals[v].width) {
+        case 1: scatter_col<uint8_t, RPT>(A.vals[v], src, gdst, srow); break;
+        case 2: scatter_col<uint16_t, RPT>(A.vals[v], src, gdst, srow); break;
+        case 4: scatter_col<uint32_t, RPT>(A.vals[v], src, gdst, srow); break;
+        default: scatter_col<uint64_t, RPT>(A.vals[v], src, gdst, srow); break;
       }
-      if (any_bits) A.bits[g] = (uint8_t)vb;
+      if (!any_bits) continue;
+      if (S.val_mask[v] < 0) {
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) vb[k] |= 1u << v;
+      } else {
+        const uint8_t* m = sm + S.soff[S.val_mask[v]];
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) vb[k] |= (uint32_t)staged_valid(m, srow[k]) << v;
+      }
+    }
+    if (any_bits) {
+#pragma unroll
+      for (int k = 0; k < RPT; ++k)
+        if (gdst[k] >= 0) A.bits[gdst[k]] = (uint8_t)vb[k];
     }
     __syncthreads();
     // the value group is free: the next full tile's values land during its A-C
@@ -416,6 +452,8 @@ inline bool part_scatter_bulk_ok(const Plan& P, int T, StageSpec& S)
     if (S.val_data[v] == -2 || S.val_mask[v] == -2) return false;
   }
   S.narr = a;
+  S.key8 = P.num_keys == 1 && P.keys[0].width == 8 && P.keys[0].mask == nullptr && P.keys[0].word == 0 &&
+           P.keys[0].shift == 0 && (P.keys[0].cat == CAT_SIGNED || P.keys[0].cat == CAT_UNSIGNED);
   S.stage_bytes = (int32_t)off;
   S.tx_bytes[0] = (int32_t)tx[0];
   S.tx_bytes[1] = (int32_t)tx[1];

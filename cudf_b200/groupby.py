@@ -83,9 +83,10 @@ class GroupBy:
 
     def set_tuning(self, block=-1, blocks_per_sm=-1, smem_bytes=-1, smem_fill_pct=-1,
                    smem_max_groups=-1, load_factor_pct=-1, force_mode=-2, groups_hint=-1, profile=-1,
-                   scatter=-1, pass2=-1, part_fill_pct=-1):
+                   scatter=-1, pass2=-1, part_fill_pct=-1, wagg_pct=-1):
         t = _lib.GbTuning(block, blocks_per_sm, smem_bytes, smem_fill_pct, smem_max_groups,
-                          load_factor_pct, force_mode, groups_hint, profile, scatter, pass2, part_fill_pct)
+                          load_factor_pct, force_mode, groups_hint, profile, scatter, pass2, part_fill_pct,
+                          wagg_pct)
         _lib.check(_lib.lib().gb_set_tuning(self._h, ctypes.byref(t)))
         return self
 

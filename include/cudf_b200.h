@@ -144,13 +144,19 @@ typedef struct gb_tuning {
                                shared memory by bulk copies when every column allows it (16-byte
                                aligned rows), else 0; 0-6 the per-thread launch shapes, threads x
                                rows per thread: 0 512x8, 1 256x16, 2 512x16, 3 1024x8, 4 512x8 with
-                               the next column's loads issued early, 5 1024x4, 6 256x8 */
+                               the next column's loads issued early, 5 1024x4, 6 256x8; 8 as 7 with
+                               2048-row tiles, two CTAs per SM */
   int32_t pass2;            /* partitioned pass 2: 1 per-row shared reductions (default); 0 (or 2)
                                chunks counting-sorted by slot, 512 threads x 4 rows; 3 sorted,
-                               256 threads x 8 rows */
+                               256 threads x 8 rows; 4 per-row, 512 threads x 2 rows (plans of
+                               up to four value columns, else as 1) */
   int32_t part_fill_pct;    /* partitioned mode: expected groups per partition as a percentage of
                                the pass-2 shared table's slots (default 70; sets the partition
                                count, a power of two) */
+  int32_t wagg_pct;         /* partitioned pass 2: a partition holding more rows than this percentage
+                               of the average partition (a heavy key) has the rows of one slot
+                               combined per warp before each shared update (default 125; 0: every
+                               partition); negative: unset */
 } gb_tuning;
 
 /* What the last gb_aggregate on a handle did. */
@@ -173,7 +179,8 @@ GB_API int gb_set_tuning(gb_handle* handle, const gb_tuning* tuning);
  * rule with rows <= max_rows, groups <= max_groups and a matching key width,
  * and applies the rule's
  * set fields (block, blocks_per_sm, smem_bytes, smem_fill_pct, smem_max_groups,
- * load_factor_pct, force_mode, scatter, pass2) except those its handle set with
+ * load_factor_pct, force_mode, scatter, pass2, part_fill_pct, wagg_pct) except those its
+ * handle set with
  * gb_set_tuning.  Replaces all rules; NULL/0 clears them.  The rules come
  * from cudf_b200.autotune, which times the candidates per bucket. */
 typedef struct gb_tuning_rule {

@@ -11,6 +11,14 @@ from parity import run_both
 pytestmark = pytest.mark.gpu
 
 
+# pass-2 settings: sorted chunks (512x4, 256x8), per-row updates (1024x1 and
+# 512x2 rows) with the
+# warp-combining kernel for heavy partitions only (default), for every
+# partition, and for split partitions only
+PASS2 = [{"pass2": 0}, {"pass2": 1}, {"pass2": 3}, {"pass2": 4}, {"pass2": 1, "wagg_pct": 0}, {"pass2": 1, "wagg_pct": 100000}]
+PASS2_ROW = [{"pass2": 0}, {"pass2": 1}, {"pass2": 4}, {"pass2": 1, "wagg_pct": 0}]
+
+
 def _cb():
     import cudf_b200 as cb
     from cudf_b200 import aggregation as agg
@@ -208,7 +216,7 @@ def test_config_shapes_medium(n, card, nulls):
               (cb.Column.from_numpy(v3, masks[2]), aggs)])
 
 
-@pytest.mark.parametrize("scatter", [0, 1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("scatter", [0, 1, 2, 3, 4, 5, 6, 7, 8])
 @pytest.mark.parametrize("nulls", [False, True])
 @pytest.mark.parametrize("two_word", [False, True])
 def test_partitioned_mode(nulls, two_word, scatter):
@@ -232,7 +240,7 @@ def test_partitioned_mode(nulls, two_word, scatter):
     assert gb.stats()["mode"] == 2
 
 
-@pytest.mark.parametrize("pass2", [0, 1, 3])
+@pytest.mark.parametrize("pass2", PASS2)
 @pytest.mark.parametrize("nulls", [False, True])
 @pytest.mark.parametrize("two_word", [False, True])
 def test_partitioned_pass2_variants(nulls, two_word, pass2):
@@ -255,7 +263,7 @@ def test_partitioned_pass2_variants(nulls, two_word, pass2):
     gb, *_ = run_both(keys, [(cb.Column.from_numpy(v1, ms[0]), aggs), (cb.Column.from_numpy(v2, ms[1]), aggs),
                              (cb.Column.from_numpy(v3, ms[2]), aggs + [agg.count(cb.NullPolicy.INCLUDE)]),
                              (cb.Column.from_numpy(v4, ms[3]), aggs + [agg.sum_of_squares()])],
-                      include_null_keys=two_word, tuning={"force_mode": 2, "pass2": pass2})
+                      include_null_keys=two_word, tuning={"force_mode": 2, **pass2})
     assert gb.stats()["mode"] == 2
 
 
@@ -269,8 +277,8 @@ def test_partitioned_mode_is_chosen_for_many_groups():
     assert gb.stats()["mode"] == 2
 
 
-@pytest.mark.parametrize("pass2", [0, 1, 3])
-@pytest.mark.parametrize("scatter", [0, 1])
+@pytest.mark.parametrize("pass2", PASS2)
+@pytest.mark.parametrize("scatter", [0, 1, 7, 8])
 def test_partitioned_spill_when_groups_underestimated(scatter, pass2):
     cb, agg = _cb()
     rng = np.random.default_rng(33)
@@ -281,11 +289,11 @@ def test_partitioned_spill_when_groups_underestimated(scatter, pass2):
     f = rng.random(n).astype(np.float32)
     run_both([cb.Column.from_numpy(key)], [(cb.Column.from_numpy(v), [agg.sum(), agg.count(), agg.min()]),
                                            (cb.Column.from_numpy(f, rng.random(n) > 0.2), [agg.mean(), agg.max()])],
-             tuning={"force_mode": 2, "groups_hint": 1000, "scatter": scatter, "pass2": pass2})
+             tuning={"force_mode": 2, "groups_hint": 1000, "scatter": scatter, **pass2})
 
 
-@pytest.mark.parametrize("pass2", [0, 1, 3])
-@pytest.mark.parametrize("scatter", [0, 1])
+@pytest.mark.parametrize("pass2", PASS2)
+@pytest.mark.parametrize("scatter", [0, 1, 7, 8])
 def test_partitioned_all_ones_key_heavy(scatter, pass2):
     """40% of the rows carry the all-ones key: one partition aggregates them in
     its dedicated shared slot, merged into the global table's slot at flush."""
@@ -299,11 +307,11 @@ def test_partitioned_all_ones_key_heavy(scatter, pass2):
     gb, *_ = run_both([cb.Column.from_numpy(key)],
                       [(cb.Column.from_numpy(v, rng.random(n) > 0.1), [agg.sum(), agg.count(), agg.min(), agg.max()]),
                        (cb.Column.from_numpy(d, rng.random(n) > 0.1), [agg.mean(), agg.min(), agg.max()])],
-                      tuning={"force_mode": 2, "scatter": scatter, "pass2": pass2})
+                      tuning={"force_mode": 2, "scatter": scatter, **pass2})
     assert gb.stats()["mode"] == 2
 
 
-@pytest.mark.parametrize("pass2", [0, 1, 3])
+@pytest.mark.parametrize("pass2", PASS2)
 def test_partitioned_skew_splits_heavy_partitions(pass2):
     """Zipf(1.3) keys: a few keys hold a large share of the rows; their
     partitions are cut into row ranges whose tables merge globally."""
@@ -313,11 +321,11 @@ def test_partitioned_skew_splits_heavy_partitions(pass2):
     key = (rng.zipf(1.3, n) % 1_000_003).astype(np.int64)
     v = rng.integers(0, 1000, n).astype(np.int64)
     gb, *_ = run_both([cb.Column.from_numpy(key)], [(cb.Column.from_numpy(v), [agg.sum(), agg.count(), agg.max()])],
-                      tuning={"force_mode": 2, "pass2": pass2})
+                      tuning={"force_mode": 2, **pass2})
     assert gb.stats()["mode"] == 2
 
 
-@pytest.mark.parametrize("pass2", [0, 1, 3])
+@pytest.mark.parametrize("pass2", PASS2)
 @pytest.mark.parametrize("hot_frac", [0.5, 0.95])
 def test_partitioned_hot_key_warp_combined_updates(hot_frac, pass2):
     """One key holds most rows: its partition is split and each warp combines
@@ -342,13 +350,13 @@ def test_partitioned_hot_key_warp_combined_updates(hot_frac, pass2):
     reqs = []
     for (v, m), t in zip(cols, types):
         reqs.append((cb.Column.from_numpy(v, m, t) if t is not None else cb.Column.from_numpy(v, m), aggs))
-    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs[:4], tuning={"force_mode": 2, "pass2": pass2})
+    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs[:4], tuning={"force_mode": 2, **pass2})
     assert gb.stats()["mode"] == 2
-    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs[4:], tuning={"force_mode": 2, "pass2": pass2})
+    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs[4:], tuning={"force_mode": 2, **pass2})
     assert gb.stats()["mode"] == 2
 
 
-@pytest.mark.parametrize("pass2", [0, 1])
+@pytest.mark.parametrize("pass2", PASS2_ROW)
 @pytest.mark.parametrize("include", [False, True])
 def test_zipf_pairs_two_word_keys(include, pass2):
     """The shape of the high-cardinality benchmark at 4M rows: (int32, int64)
@@ -365,7 +373,7 @@ def test_zipf_pairs_two_word_keys(include, pass2):
     vf = rng.random(n)
     aggs = [agg.sum(), agg.count(), agg.max()]
     gb, *_ = run_both([k1, k2], [(cb.Column.from_numpy(vi), aggs), (cb.Column.from_numpy(vf), aggs)],
-                      include_null_keys=include, tuning={"pass2": pass2})
+                      include_null_keys=include, tuning={**pass2})
     assert gb.stats()["mode"] == 2
 
 
@@ -499,7 +507,7 @@ def test_shared_stage_row_ranges_match_both_kernels(policy):
     assert gb.stats()["mode"] == 1
 
 
-@pytest.mark.parametrize("pass2", [0, 1])
+@pytest.mark.parametrize("pass2", PASS2_ROW)
 def test_partitioned_many_partitions_wide_slots(pass2):
     """Wide slots (eight value columns) leave ~1000 slots per shared table, so
     3.5M groups need 8192 partitions; every group and value must still match."""
@@ -512,5 +520,5 @@ def test_partitioned_many_partitions_wide_slots(pass2):
         v = rng.integers(-10**9, 10**9, n).astype(np.int64)
         reqs.append((cb.Column.from_numpy(v, rng.random(n) > 0.1 if i % 2 else None),
                      [agg.sum(), agg.min(), agg.max()]))
-    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs, tuning={"pass2": pass2})
+    gb, *_ = run_both([cb.Column.from_numpy(key)], reqs, tuning={**pass2})
     assert gb.stats()["mode"] == 2
