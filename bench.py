@@ -283,9 +283,10 @@ def run_engine(args):
         from cudf_b200.types import Kind
         kinds = [Kind.SUM, Kind.COUNT_VALID, Kind.MIN, Kind.MAX, Kind.MEAN]
         dkeys = [(key, None, TypeId.INT64)]
-        dreqs = [((vals[0], cb.column.unpack_mask(masks[0], n), TypeId.INT64), kinds),
-                 ((vals[1], cb.column.unpack_mask(masks[1], n), TypeId.FLOAT64), kinds),
-                 ((vals[2], cb.column.unpack_mask(masks[2], n), TypeId.FLOAT32), kinds)]
+        # the packed validity words go to the engine as they are
+        dreqs = [((vals[0], masks[0], TypeId.INT64), kinds),
+                 ((vals[1], masks[1], TypeId.FLOAT64), kinds),
+                 ((vals[2], masks[2], TypeId.FLOAT32), kinds)]
 
         class _Res:
             def __init__(self, k):
@@ -384,7 +385,7 @@ def run_engine(args):
             types = (TypeId.INT64, TypeId.FLOAT64, TypeId.FLOAT32)
             mk, mres = distributed_groupby(
                 [(t[0], None, TypeId.INT64)],
-                [((t[1 + i], cb.column.unpack_mask(t[4 + i], n), types[i]), kinds) for i in range(3)])
+                [((t[1 + i], t[4 + i], types[i]), kinds) for i in range(3)])
             outs = [d for d, _, _ in mk] + [x for per in mres for pair in per for x in pair if x is not None]
         else:
             uk2, res2 = cb.GroupBy(cb.Table([bufs[b][1]])).aggregate(bufs[b][2], stream=stream)

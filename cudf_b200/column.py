@@ -97,7 +97,12 @@ class Column:
         if type_id is None:
             type_id = FROM_TORCH[t.dtype]
         t = t.contiguous()
-        mask = None if valid is None else pack_mask(valid.to(device=t.device, dtype=torch.bool))
+        if valid is None:
+            mask = None
+        elif valid.dtype in (torch.int32, torch.uint32) and valid.numel() == (t.shape[0] + 31) // 32:
+            mask = valid.to(t.device).contiguous()  # packed validity words, LSB first
+        else:
+            mask = pack_mask(valid.to(device=t.device, dtype=torch.bool))
         return Column(type_id, t, mask)
 
     @staticmethod

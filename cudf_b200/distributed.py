@@ -22,6 +22,7 @@ from __future__ import annotations
 
 from typing import Callable, List, Optional, Sequence, Tuple
 
+import numpy as np
 import torch
 import torch.distributed as dist
 
@@ -92,21 +93,38 @@ def owner_rank(key_cols: Sequence[Tuple[torch.Tensor, Optional[torch.Tensor], in
 
 
 def _exchange(tensors: List[torch.Tensor], dest: torch.Tensor, world: int, group=None) -> List[torch.Tensor]:
-    """Sends row i of every tensor to rank dest[i] (one all-to-all per tensor)."""
+    """Sends row i of every tensor to rank dest[i].  The tensors travel as one
+    row-major byte matrix (each row: every tensor's bytes of that row, bool
+    as one byte), gathered into destination order once, so the exchange is
+    two collectives whatever the number of columns: the per-rank row counts,
+    then the payload.  The counts are read on the host (one synchronisation:
+    the payload's split sizes)."""
+    n = int(dest.shape[0])
     order = torch.argsort(dest, stable=True)
     counts = torch.bincount(dest, minlength=world).to(torch.int64)
     recv_counts = torch.empty_like(counts)
     dist.all_to_all_single(recv_counts, counts, group=group)
-    send_splits = counts.tolist()
-    recv_splits = recv_counts.tolist()
-    out = []
+    both = torch.stack([counts, recv_counts]).cpu()
+    send_splits, recv_splits = both[0].tolist(), both[1].tolist()
+    parts, widths = [], []
     for t in tensors:
-        src = t[order].contiguous()
-        if src.dtype == torch.bool:
-            src = src.to(torch.uint8)
-        r = torch.empty((sum(recv_splits),) + tuple(src.shape[1:]), dtype=src.dtype, device=src.device)
-        dist.all_to_all_single(r, src, recv_splits, send_splits, group=group)
-        out.append(r.to(torch.bool) if t.dtype == torch.bool else r)
+        u = t.to(torch.uint8) if t.dtype == torch.bool else t
+        w = u.element_size() * (int(np.prod(u.shape[1:])) if u.dim() > 1 else 1)
+        parts.append(u.contiguous().view(torch.uint8).reshape(n, w) if n else
+                     torch.empty((0, w), dtype=torch.uint8, device=dest.device))
+        widths.append(w)
+    rows = torch.cat(parts, dim=1)[order].contiguous() if parts else torch.empty((n, 0), dtype=torch.uint8,
+                                                                                   device=dest.device)
+    recv = torch.empty((sum(recv_splits), rows.shape[1]), dtype=torch.uint8, device=rows.device)
+    dist.all_to_all_single(recv, rows, recv_splits, send_splits, group=group)
+    out, at = [], 0
+    for t, w in zip(tensors, widths):
+        b = recv[:, at:at + w].contiguous()
+        at += w
+        if t.dtype == torch.bool:
+            out.append(b.reshape(-1) != 0)
+        else:
+            out.append(b.view(t.dtype).reshape((-1,) + tuple(t.shape[1:])))
     return out
 
 
@@ -206,8 +224,10 @@ def finalize_partials(requests, merged):
 def distributed_groupby(keys, requests, null_handling: NullPolicy = NullPolicy.EXCLUDE, group=None,
                         local_aggregate: Optional[Callable] = None):
     """keys: [(data, valid|None, type_id)] of this rank's shard; requests:
-    [((data, valid|None, type_id), [Kind])].  Returns (keys, results) of the
-    groups this rank owns, results[r][j] = (values, valid|None)."""
+    [((data, valid|None, type_id), [Kind])]; `valid` is a bool per row or
+    the packed 32-bit validity words (LSB first) the engine's columns carry.
+    Returns (keys, results) of the groups this rank owns,
+    results[r][j] = (values, valid|None)."""
     local = local_aggregate or engine_local_aggregate
     world = dist.get_world_size(group)
     # 1. partial aggregation of the shard

@@ -138,3 +138,65 @@ def test_owner_rank_is_consistent_and_balanced():
     assert counts.min() > 0.9 * counts.mean()
     fr = owner_rank([(f, None, O.FLOAT64)], 8)
     assert fr[0] == fr[1] and fr[2] == fr[3]  # -0.0 == +0.0, all NaNs one key
+
+
+def _exchange_worker(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from cudf_b200.distributed import _exchange
+        rng = np.random.default_rng(100 + rank)
+        n = 0 if rank == 1 else 37  # rank 1 sends nothing
+        dest = torch.from_numpy(rng.integers(0, world, n).astype(np.int64))
+        cols = [torch.from_numpy(rng.integers(-2**62, 2**62, n).astype(np.int64)),
+                torch.from_numpy(rng.random(n).astype(np.float32)),
+                torch.from_numpy(rng.random(n) > 0.5),
+                torch.from_numpy(rng.integers(0, 100, (n, 3)).astype(np.int16))]
+        got = _exchange(cols, dest, world)
+        sent = [(dest.numpy(), [c.numpy() for c in cols])]
+        everything = [None] * world
+        dist.all_gather_object(everything, (rank, sent, [g.numpy() for g in got]))
+        if rank == 0:
+            q.put(everything)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_exchange_packs_every_column_into_one_payload():
+    """Rows reach the rank named by `dest` with every column intact (int64,
+    float32, bool, a 2-D int16 block), in the senders' rank order and each
+    sender's row order; a rank with no rows takes part."""
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_exchange_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in ps:
+        p.start()
+    everything = q.get(timeout=120)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    by_rank = {r: (sent, got) for r, sent, got in everything}
+    for dst in range(world):
+        expect = [[] for _ in range(4)]
+        for src in range(world):
+            d, cols = by_rank[src][0][0]
+            for i, c in enumerate(cols):
+                expect[i].append(c[d == dst])
+        got = by_rank[dst][1]
+        for i in range(4):
+            e = np.concatenate(expect[i]) if expect[i] else np.zeros(0)
+            assert got[i].dtype == e.dtype and got[i].shape == e.shape
+            assert np.array_equal(got[i], e)
+
+
+def test_packed_validity_words_are_taken_as_the_mask():
+    from cudf_b200.column import Column, pack_mask
+    valid = torch.from_numpy(np.random.default_rng(3).random(70) > 0.3)
+    data = torch.arange(70, dtype=torch.int64)
+    a = Column.from_tensor(data, valid)
+    b = Column.from_tensor(data, pack_mask(valid))
+    assert torch.equal(a.mask, b.mask)
+    assert torch.equal(b.valid(), valid)
