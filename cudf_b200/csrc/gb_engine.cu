@@ -864,6 +864,12 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
         }
         if (pass == 0) nwagg = (int)items.size();
       }
+      // CTAs claim items in order: largest first within each launch, so the
+      // launch does not end waiting on one long item taken last
+      auto rows_of = [&](const PartItem& it) { return it.merge ? it.end - it.begin : prows[it.part]; };
+      auto larger = [&](const PartItem& x, const PartItem& y) { return rows_of(x) > rows_of(y); };
+      std::stable_sort(items.begin(), items.begin() + nwagg, larger);
+      std::stable_sort(items.begin() + nwagg, items.end(), larger);
     }
     PartItem* d_items = (PartItem*)S.get(sizeof(PartItem) * items.size());
     ck(cudaMemcpyAsync(d_items, items.data(), sizeof(PartItem) * items.size(), cudaMemcpyHostToDevice, stream), "h2d");
