@@ -45,16 +45,16 @@ CPU_SAMPLE_ROWS = N_ROWS
 # Kernels whose device time the roofline covers, by engine mode (0 global
 # table, 1 shared-memory stage, 2 hash-partitioned two-pass).
 KERNELS_BY_MODE = {0: "k_aggregate<false>", 1: "k_aggregate<true>",
-                   2: "k_part_scatter + k_part_aggregate"}
+                   2: "k_part_scatter_bulk + k_part_aggregate"}
 # DRAM bytes (read + write) of those kernels per launch, from an ncu capture
 # of a smaller case of the same workload scaled up; the capture command and
 # the per-kernel figures are in profiles/.
 # Mode 2: (bytes per row, bytes per group); the partitioned copy is written
 # and read once, and the dense slots are written once per group.
-TRAFFIC_MODEL = {2: (90.07, 75.1)}
+TRAFFIC_MODEL = {2: (84.65, 76.1)}
 TRAFFIC_SOURCE = {2: "ncu dram__bytes_read.sum + dram__bytes_write.sum of both kernels on the 20M-row "
                      "case, scaled by rows (and by groups for the dense-slot writes); "
-                     "profiles/k_part_scatter_k_part_aggregate_20M.md"}
+                     "profiles/k_part_scatter_bulk_k_part_aggregate_20M.md"}
 
 
 def algorithmic_bytes(n_rows: int, n_groups: int) -> tuple[float, float]:

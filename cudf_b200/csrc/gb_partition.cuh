@@ -348,17 +348,38 @@ __device__ __forceinline__ uint8_t* smem_slot(uint8_t* smem, int stride, uint32_
   uint32_t i = (uint32_t)(((uint64_t)(uint32_t)h * scap) >> 32);
   if (words == 1) {
     if (w0 == kEmpty) return nullptr;
-    for (int p = 0; p < 64; ++p) {
-      unsigned long long* kp = (unsigned long long*)(smem + (size_t)i * stride);
-      uint64_t cur = *(volatile unsigned long long*)kp;
-      if (cur == w0) return (uint8_t*)kp;
-      if (cur == kEmpty) {
-        if (*(volatile unsigned int*)s_used >= (unsigned)sfill) return nullptr;
-        uint64_t old = atomicCAS(kp, kEmpty, w0);
-        if (old == kEmpty) { atomicAdd(s_used, 1u); return (uint8_t*)kp; }
-        if (old == w0) return (uint8_t*)kp;
+    // two consecutive slots per step, both keys loaded together: a warp
+    // runs as many steps as its longest probe, so halving the steps halves
+    // the divergent tail.  A key sits at or before the first empty slot of
+    // its sequence (no deletions), so an empty first slot is claimed before
+    // the second is looked at.
+    auto claim = [&](unsigned long long* kp) -> int {  // 1 mine, 0 taken by another key, -1 full
+      if (*(volatile unsigned int*)s_used >= (unsigned)sfill) return -1;
+      const uint64_t old = atomicCAS(kp, kEmpty, w0);
+      if (old == kEmpty) { atomicAdd(s_used, 1u); return 1; }
+      return old == w0 ? 1 : 0;
+    };
+    for (int p = 0; p < 64; p += 2) {
+      const uint32_t i1 = i + 1 == scap ? 0 : i + 1;
+      unsigned long long* k0p = (unsigned long long*)(smem + (size_t)i * stride);
+      unsigned long long* k1p = (unsigned long long*)(smem + (size_t)i1 * stride);
+      const uint64_t c0 = *(volatile unsigned long long*)k0p;
+      const uint64_t c1 = *(volatile unsigned long long*)k1p;
+      if (c0 == w0) return (uint8_t*)k0p;
+      if (c0 == kEmpty) {
+        const int r = claim(k0p);
+        if (r > 0) return (uint8_t*)k0p;
+        if (r < 0) return nullptr;
+        i = i1;  // taken meanwhile: the sequence continues at the second slot
+        continue;
       }
-      i = i + 1 == scap ? 0 : i + 1;
+      if (c1 == w0) return (uint8_t*)k1p;
+      if (c1 == kEmpty) {
+        const int r = claim(k1p);
+        if (r > 0) return (uint8_t*)k1p;
+        if (r < 0) return nullptr;
+      }
+      i = i1 + 1 == scap ? 0 : i1 + 1;
     }
     return nullptr;
   }
