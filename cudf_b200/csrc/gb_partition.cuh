@@ -383,19 +383,38 @@ __device__ __forceinline__ uint8_t* smem_slot(uint8_t* smem, int stride, uint32_
     }
     return nullptr;
   }
+  // two-word keys: an empty slot has the top bit of its second word set
+  // (never set in a packed key); a first word of all ones is a valid key
+  // and is matched through the compare-and-swap.  Two slots per step, as for
+  // one-word keys.
   unsigned __int128 want = ((unsigned __int128)w1 << 64) | w0;
   const unsigned __int128 empty = ~(unsigned __int128)0;
-  for (int p = 0; p < 64; ++p) {
-    unsigned __int128* kp = (unsigned __int128*)(smem + (size_t)i * stride);
-    ulonglong2 cur = vload2(kp);
-    if (cur.x == w0 && cur.y == w1 && w0 != kEmpty) return (uint8_t*)kp;
+  // 1: the key's slot, 0: another key's, -1: table at its fill limit
+  auto look = [&](unsigned __int128* kp, ulonglong2 cur) -> int {
+    if (cur.x == w0 && cur.y == w1 && w0 != kEmpty) return 1;
     if ((cur.y >> 63) || cur.x == kEmpty) {
-      if ((cur.y >> 63) && *(volatile unsigned int*)s_used >= (unsigned)sfill) return nullptr;
+      if ((cur.y >> 63) && *(volatile unsigned int*)s_used >= (unsigned)sfill) return -1;
       unsigned __int128 old = atomicCAS(kp, empty, want);
-      if (old == empty) { atomicAdd(s_used, 1u); return (uint8_t*)kp; }
-      if (old == want) return (uint8_t*)kp;
+      if (old == empty) { atomicAdd(s_used, 1u); return 1; }
+      if (old == want) return 1;
     }
-    i = i + 1 == scap ? 0 : i + 1;
+    return 0;
+  };
+  for (int p = 0; p < 64; p += 2) {
+    const uint32_t i1 = i + 1 == scap ? 0 : i + 1;
+    unsigned __int128* kp0 = (unsigned __int128*)(smem + (size_t)i * stride);
+    unsigned __int128* kp1 = (unsigned __int128*)(smem + (size_t)i1 * stride);
+    const ulonglong2 c0 = vload2(kp0);
+    const ulonglong2 c1 = vload2(kp1);
+    // the first slot is settled (ours, or another key's) before the second
+    // is looked at; a second slot seen empty is claimed by compare-and-swap
+    int r = look(kp0, c0);
+    if (r > 0) return (uint8_t*)kp0;
+    if (r < 0) return nullptr;
+    r = look(kp1, c1);
+    if (r > 0) return (uint8_t*)kp1;
+    if (r < 0) return nullptr;
+    i = i1 + 1 == scap ? 0 : i1 + 1;
   }
   return nullptr;
 }
