@@ -51,7 +51,7 @@ KERNELS_BY_MODE = {0: "k_aggregate<false>", 1: "k_aggregate<true>",
 # the per-kernel figures are in profiles/.
 # Mode 2: (bytes per row, bytes per group); the partitioned copy is written
 # and read once, and the dense slots are written once per group.
-TRAFFIC_MODEL = {2: (84.65, 76.1)}
+TRAFFIC_MODEL = {2: (84.93, 75.1)}
 TRAFFIC_SOURCE = {2: "ncu dram__bytes_read.sum + dram__bytes_write.sum of both kernels on the 20M-row "
                      "case, scaled by rows (and by groups for the dense-slot writes); "
                      "profiles/k_part_scatter_bulk_k_part_aggregate_20M.md"}

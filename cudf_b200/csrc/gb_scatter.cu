@@ -11,6 +11,7 @@ namespace {
 // tile's layout fits shared memory, else 2048-row tiles with two 512-thread
 // CTAs per SM.
 constexpr int kBigRows = 4096, kBigThreads = 1024;
+constexpr int kMidRows = 3072;  // 1024 threads, 3 rows each
 constexpr int kRows = 2048, kThreads = 512;
 }  // namespace
 
@@ -19,8 +20,13 @@ size_t part_scatter_bulk_plan(const Plan& P, int nparts, int smem_optin, void* s
   StageSpec& S = *(StageSpec*)spec_out;
   // static shared memory of the kernel (barriers, scan temporaries) plus slack
   const size_t limit = (size_t)smem_optin - 8192;
-  if (!small_only && part_scatter_bulk_ok(P, kBigRows, S)) {
-    const size_t sm = part_scatter_bulk_smem(S, P.key_words, kBigRows, nparts);
+  // one 1024-thread CTA per SM on 4096-row tiles where they fit, else on
+  // 3072-row tiles (wide keys with many partitions), else two CTAs of 512 on
+  // 2048-row tiles: the per-tile partition work is paid per tile, so the
+  // largest tile that fits wins
+  for (int T : {kBigRows, kMidRows}) {
+    if (small_only || !part_scatter_bulk_ok(P, T, S)) continue;
+    const size_t sm = part_scatter_bulk_smem(S, P.key_words, T, nparts);
     if (sm <= limit) return sm;
   }
   if (!part_scatter_bulk_ok(P, kRows, S)) return 0;
@@ -46,6 +52,11 @@ void launch_part_scatter_bulk(const Plan& P, const PartArgs& A, const void* spec
 {
   const StageSpec& S = *(const StageSpec*)spec;
   const bool is_big = S.tile_rows == kBigRows;
+  if (S.tile_rows == kMidRows) {
+    if (P.key_words == 1) launch_bulk<1, kBigThreads, kMidRows, 1>(P, A, S, smem, stream);
+    else launch_bulk<2, kBigThreads, kMidRows, 1>(P, A, S, smem, stream);
+    return;
+  }
   if (P.key_words == 1) {
     if (is_big) launch_bulk<1, kBigThreads, kBigRows, 1>(P, A, S, smem, stream);
     else launch_bulk<1, kThreads, kRows, 2>(P, A, S, smem, stream);

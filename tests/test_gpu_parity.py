@@ -377,6 +377,25 @@ def test_zipf_pairs_two_word_keys(include, pass2):
     assert gb.stats()["mode"] == 2
 
 
+@pytest.mark.parametrize("scatter", [7, 8])
+def test_two_word_keys_many_partitions(scatter):
+    """(int32, int64) keys with nulls over ~3M groups: 2048 partitions, too
+    many for the bulk pass's 4096-row tiles with two-word keys, so it runs on
+    3072-row tiles (scatter 7) or 2048-row tiles with two CTAs per SM (8)."""
+    cb, agg = _cb()
+    rng = np.random.default_rng(52)
+    n = 6_000_000
+    p = rng.integers(0, 3_000_000, n)
+    k1 = cb.Column.from_numpy((p // 1000).astype(np.int32), rng.random(n) >= 0.05)
+    k2 = cb.Column.from_numpy(p % 1000 * 7919, rng.random(n) >= 0.05)
+    vi = rng.integers(-10**9, 10**9, n).astype(np.int64)
+    vf = rng.normal(size=n)
+    aggs = [agg.sum(), agg.count(), agg.min(), agg.max()]
+    gb, *_ = run_both([k1, k2], [(cb.Column.from_numpy(vi), aggs), (cb.Column.from_numpy(vf), aggs)],
+                      include_null_keys=True, tuning={"force_mode": 2, "scatter": scatter})
+    assert gb.stats()["mode"] == 2
+
+
 def test_distributed_groupby_single_rank_with_engine():
     """The multi-GPU path with the engine as local aggregation (world size 1 on
     one GPU: partial aggregate, self-exchange, merge)."""
