@@ -42,9 +42,8 @@ __device__ __forceinline__ int64_t sign_extend(uint64_t bits, int width)
 // normalised key bits: all NaNs one value, -0.0 == +0.0, bool -> 0/1
 // (libcudf hashes and compares keys this way:
 //  cpp/include/cudf/hashing/detail/murmurhash3_x86_32.cuh:66-68)
-__device__ __forceinline__ uint64_t key_bits(const KeyCol& c, int64_t r)
+__device__ __forceinline__ uint64_t norm_key_bits(const KeyCol& c, uint64_t b)
 {
-  uint64_t b = load_bits(c.data, r, c.width);
   if (c.cat == CAT_F32) {
     float f = __uint_as_float((uint32_t)b);
     if (f != f) return 0x7FC00000u;
@@ -59,6 +58,10 @@ __device__ __forceinline__ uint64_t key_bits(const KeyCol& c, int64_t r)
   }
   if (c.cat == CAT_BOOL) return b != 0;
   return b;
+}
+__device__ __forceinline__ uint64_t key_bits(const KeyCol& c, int64_t r)
+{
+  return norm_key_bits(c, load_bits(c.data, r, c.width));
 }
 
 // Packs the key tuple of a row into one or two 64-bit words.  Returns false

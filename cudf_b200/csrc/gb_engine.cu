@@ -529,13 +529,15 @@ void set_tuning_rules(const std::vector<TuningRule>& rules)
   g_rules = rules;
 }
 
-int apply_tuning_rules(Options& o, int64_t rows, int64_t groups, int key_words)
+int apply_tuning_rules(Options& o, int64_t rows, int64_t groups, int key_words, uint32_t* applied)
 {
   std::lock_guard<std::mutex> lk(g_rules_mu);
+  if (applied) *applied = 0;
   for (size_t i = 0; i < g_rules.size(); ++i) {
     const TuningRule& r = g_rules[i];
     if (rows > r.max_rows || groups > r.max_groups || (r.key_words && r.key_words != key_words)) continue;
     const uint32_t m = r.mask & ~o.set_mask;
+    if (applied) *applied = m;
     if (m & OPT_BLOCK) o.block = r.opt.block;
     if (m & OPT_BPS) o.blocks_per_sm = r.opt.blocks_per_sm;
     if (m & OPT_SMEM) o.smem_bytes = r.opt.smem_bytes;
@@ -638,7 +640,25 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     nsamp = valid_rows;
   }
   st.est_groups = est;
-  st.rule = apply_tuning_rules(opt, n, est, P.key_words);
+  uint32_t rule_fields = 0;
+  st.rule = apply_tuning_rules(opt, n, est, P.key_words, &rule_fields);
+  // Many heavy hitters (a long-tailed key distribution, e.g. Zipf): besides
+  // the few partitions well above the average size, most partitions hold keys
+  // with hundreds of rows, whose lanes would queue on one shared address, so
+  // every partition combines the rows of one slot per warp first.  The sign is
+  // in the exact bucket counts: at least 32 buckets above four times the mean
+  // of the non-empty ones (uniform keys have none; one hot key makes one).
+  if (exact_buckets && !((opt.set_mask | rule_fields) & OPT_WAGG)) {
+    int64_t rows_in = 0, nonempty = 0;
+    for (auto b : buckets) {
+      rows_in += b;
+      nonempty += b > 0;
+    }
+    const double mean = nonempty ? (double)rows_in / (double)nonempty : 0.0;
+    int heavy = 0;
+    for (auto b : buckets) heavy += (double)b > 4.0 * mean;
+    if (heavy >= 32) opt.wagg_pct = 0;
+  }
   mark("estimate");
 
   // ---- mode ----

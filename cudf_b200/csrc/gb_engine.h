@@ -107,7 +107,7 @@ struct TuningRule {
 };
 void set_tuning_rules(const std::vector<TuningRule>& rules);
 // Applies the first rule matching (rows, groups) to `o`; returns its index or -1.
-int apply_tuning_rules(Options& o, int64_t rows, int64_t groups, int key_words);
+int apply_tuning_rules(Options& o, int64_t rows, int64_t groups, int key_words, uint32_t* applied = nullptr);
 
 struct Stats {
   int64_t est_groups = 0;

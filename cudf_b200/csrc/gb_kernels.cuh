@@ -440,8 +440,8 @@ static __global__ void __launch_bounds__(512) k_sketch(const __grid_constant__ P
   __syncthreads();
   const int64_t n = P.num_rows;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  auto add = [&](uint64_t h) {
-    atomicAdd(&bk[h >> (64 - kBucketBits)], 1u);
+  auto add = [&](uint64_t h, unsigned rows) {
+    atomicAdd(&bk[h >> (64 - kBucketBits)], rows);
     const uint64_t low = h << 24;
     const unsigned rank = low ? (unsigned)__clzll((long long)low) + 1u : 41u;
     atomicMax(&reg[(h >> 40) & ((1u << kHllBits) - 1)], rank);
@@ -455,14 +455,56 @@ static __global__ void __launch_bounds__(512) k_sketch(const __grid_constant__ P
 #pragma unroll
       for (int j = 0; j < 4; ++j) k[j] = __ldg(kd + row + j * stride);
 #pragma unroll
-      for (int j = 0; j < 4; ++j) add(fmix64(k[j]));
+      for (int j = 0; j < 4; ++j) add(fmix64(k[j]), 1u);
     }
-    for (; row < n; row += stride) add(fmix64(__ldg(kd + row)));
+    for (; row < n; row += stride) add(fmix64(__ldg(kd + row)), 1u);
   } else {
-    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n; row += stride) {
-      uint64_t w0, w1;
-      if (!pack_key(P, row, w0, w1)) continue;
-      add(hash_key(w0, w1, P.key_words));
+    // several key columns, nullable or floating-point keys: four rows per
+    // thread, packed column by column so that the four rows' data and mask
+    // loads of a column are in flight together (as pack_key, per row)
+    constexpr int SR = 4;
+    for (int64_t row0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row0 < n; row0 += SR * stride) {
+      uint64_t w0[SR], w1[SR];
+      bool ok[SR];
+#pragma unroll
+      for (int j = 0; j < SR; ++j) {
+        w0[j] = 0;
+        w1[j] = 0;
+        ok[j] = row0 + j * stride < n;
+      }
+#pragma unroll 1
+      for (int k = 0; k < P.num_keys; ++k) {
+        const KeyCol& c = P.keys[k];
+        uint64_t b[SR];
+        uint32_t mw[SR];
+#pragma unroll
+        for (int j = 0; j < SR; ++j) {
+          const int64_t r = row0 + j * stride + c.offset;
+          b[j] = ok[j] ? load_bits(c.data, r, c.width) : 0;
+          mw[j] = (ok[j] && c.mask) ? __ldg(c.mask + (r >> 5)) : 0xFFFFFFFFu;
+        }
+#pragma unroll
+        for (int j = 0; j < SR; ++j) {
+          if (!ok[j]) continue;
+          const int64_t r = row0 + j * stride + c.offset;
+          if (!((mw[j] >> (r & 31)) & 1u)) {
+            if (!P.include_nulls) {
+              ok[j] = false;
+              continue;
+            }
+            const uint64_t nb = 1ull << c.null_shift;
+            if (c.null_word == 0) w0[j] |= nb;
+            else w1[j] |= nb;
+            continue;
+          }
+          const uint64_t v = norm_key_bits(c, b[j]) << c.shift;
+          if (c.word == 0) w0[j] |= v;
+          else w1[j] |= v;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < SR; ++j)
+        if (ok[j]) add(hash_key(w0[j], w1[j], P.key_words), 1u);
     }
   }
   __syncthreads();

@@ -156,7 +156,9 @@ typedef struct gb_tuning {
   int32_t wagg_pct;         /* partitioned pass 2: a partition holding more rows than this percentage
                                of the average partition (a heavy key) has the rows of one slot
                                combined per warp before each shared update (default 125; 0: every
-                               partition); negative: unset */
+                               partition; when unset and the sketch finds many heavy hitters -- at
+                               least 32 of its row-count buckets above four times the mean of the
+                               non-empty ones -- every partition); negative: unset */
 } gb_tuning;
 
 /* What the last gb_aggregate on a handle did. */

@@ -82,3 +82,22 @@ int use(cudf::table_view const& keys, cudf::column_view const& vals) {
                             "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include", f],
                            capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_tuning_fields_are_range_checked_on_the_host():
+    """gb_set_tuning accepts every documented pass-2 variant (0-4) and rejects
+    the next value; the handle holds column views only, so no device is needed."""
+    import ctypes
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    col = _lib.GbColumn(4, 8, 0, 0, 0)
+    assert L.gb_create(ctypes.byref(col), 1, 0, 0, ctypes.byref(h)) == _lib.GB_OK
+    try:
+        def tuning(pass2):
+            return _lib.GbTuning(-1, -1, -1, -1, -1, -1, -2, -1, -1, -1, pass2, -1, -1)
+        for p in range(5):
+            assert L.gb_set_tuning(h, ctypes.byref(tuning(p))) == _lib.GB_OK, p
+        assert L.gb_set_tuning(h, ctypes.byref(tuning(5))) == _lib.GB_ERR_LOGIC
+        assert b"pass2" in L.gb_last_error()
+    finally:
+        L.gb_destroy(h)
