@@ -292,38 +292,65 @@ __global__ void __launch_bounds__(NT, MINB) k_part_scatter_bulk(const __grid_con
       }
       pending[0] = true;
     }
-    // B: reservations, then the scan (as k_part_scatter)
+    // B: the tile's positions (exclusive scan of the histogram) and one
+    // reservation per partition present on its region cursor.  With at most
+    // four partitions per thread the reservations are issued before the scan
+    // and their results are first used after C, so their round trip to L2
+    // overlaps the scan and the placement of the keys; with more, each is
+    // used as it returns.
+    const int q0 = threadIdx.x * per;
+    const int qe = min(A.nparts, q0 + per);
+    const bool early = per <= 4;
+    unsigned long long g4[4];
     unsigned mine = 0;
-    for (int q0 = threadIdx.x * per; q0 < min(A.nparts, (threadIdx.x + 1) * per); q0 += 4) {
-      unsigned h[4];
-      unsigned long long g[4];
+    if (early) {
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const int q = q0 + j;
-        h[j] = (j < per && q < min(A.nparts, (threadIdx.x + 1) * per)) ? hist[q] : 0u;
-        g[j] = h[j] ? atomicAdd(&A.cursor[q], (unsigned long long)h[j]) : 0ull;
-        mine += h[j];
+        const unsigned h = q < qe ? hist[q] : 0u;
+        g4[j] = h ? atomicAdd(&A.cursor[q], (unsigned long long)h) : 0ull;
+        mine += h;
       }
+    } else {
+      for (int qa = q0; qa < qe; qa += 4) {
+        unsigned h[4];
+        unsigned long long g[4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int q = q0 + j;
-        if (!h[j]) continue;
-        const long long room = (long long)A.end[q] - (long long)g[j];
-        if ((long long)h[j] > room) atomicOr(A.counters + 5, 1u);
-        delta[q] = (long long)g[j];
-        send[q] = room <= 0 ? 0u : (unsigned)min((long long)h[j], room);
+        for (int j = 0; j < 4; ++j) {
+          const int q = qa + j;
+          h[j] = q < qe ? hist[q] : 0u;
+          g[j] = h[j] ? atomicAdd(&A.cursor[q], (unsigned long long)h[j]) : 0ull;
+          mine += h[j];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int q = qa + j;
+          if (!h[j]) continue;
+          const long long room = (long long)A.end[q] - (long long)g[j];
+          if ((long long)h[j] > room) atomicOr(A.counters + 5, 1u);
+          delta[q] = (long long)g[j];
+          send[q] = room <= 0 ? 0u : (unsigned)min((long long)h[j], room);
+        }
       }
     }
     unsigned pre, total;
     Scan(scan_tmp).ExclusiveSum(mine, pre, total);
-    for (int q = threadIdx.x * per; q < min(A.nparts, (threadIdx.x + 1) * per); ++q) {
-      const unsigned h = hist[q];
-      if (h) {
-        delta[q] -= (long long)pre;
-        send[q] += pre;
+    if (early) {
+      for (int q = q0; q < qe; ++q) {
+        const unsigned h = hist[q];
+        hist[q] = pre;
+        pre += h;
       }
-      hist[q] = pre;
-      pre += h;
+    } else {
+      for (int q = q0; q < qe; ++q) {
+        const unsigned h = hist[q];
+        if (h) {
+          delta[q] -= (long long)pre;
+          send[q] += pre;
+        }
+        hist[q] = pre;
+        pre += h;
+      }
     }
     if (threadIdx.x == 0) s_valid = total;
     __syncthreads();
@@ -338,6 +365,23 @@ __global__ void __launch_bounds__(NT, MINB) k_part_scatter_bulk(const __grid_con
       psort[s] = (uint16_t)p;
       kst[KW * s] = kw0[k];
       if (KW == 2) kst[2 * s + 1] = kw1[k];
+    }
+    // the early reservations have returned by now: destinations and bounds
+    // per partition (read by D after the next barrier); a partition's tile
+    // position and row count come back from the scanned histogram
+    if (early) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int q = q0 + j;
+        if (q >= qe) break;
+        const unsigned pq = hist[q];
+        const unsigned h = (q + 1 < A.nparts ? hist[q + 1] : s_valid) - pq;
+        if (!h) continue;
+        const long long room = (long long)A.end[q] - (long long)g4[j];
+        if ((long long)h > room) atomicOr(A.counters + 5, 1u);
+        delta[q] = (long long)g4[j] - (long long)pq;
+        send[q] = pq + (room <= 0 ? 0u : (unsigned)min((long long)h, room));
+      }
     }
     if (cnt == T) wait_group(1);  // issued after the previous tile's write-out
     __syncthreads();
