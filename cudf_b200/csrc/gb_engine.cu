@@ -617,8 +617,10 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
     {
       const size_t sm = sketch_smem();
       allow_max_smem((const void*)k_sketch);
+      // at least 16Ki rows per CTA: each CTA clears and merges 80 KB of
+      // shared counters, which dominates on small inputs
       int grid = grid_for((const void*)k_sketch, 512, sm, 0);
-      grid = (int)std::min<int64_t>(grid, (n + 511) / 512);
+      grid = (int)std::min<int64_t>(grid, (n + 16383) / 16384);
       k_sketch<<<grid, 512, sm, stream>>>(P, hll, bk);
     }
     st.kernels += 1;

@@ -501,9 +501,11 @@ __device__ __forceinline__ int p2_claim(const PartArgs& A, uint8_t* smem, int sc
     *s_used = 0;
     *s_spill = 0;
   }
-  for (int i = threadIdx.x; i < scap * nw; i += NT) {
-    int s = i / nw;
-    *(unsigned long long*)(smem + (size_t)s * nw * 8 + (i - s * nw) * 8) = tmpl.w[i - s * nw];
+  // word by word: every thread reads the same template word (no divergent
+  // parameter loads, no division by the slot width)
+  for (int w = 0; w < nw; ++w) {
+    const unsigned long long t = tmpl.w[w];
+    for (int s = threadIdx.x; s < scap; s += NT) *(unsigned long long*)(smem + ((size_t)s * nw + w) * 8) = t;
   }
   __syncthreads();
   return *s_part;
@@ -590,14 +592,11 @@ template <int CAT, int W, int R, int MAXV, bool WAGG>
 __device__ __forceinline__ void p2_column(const ValCol& c, const uint32_t (&sa)[R], const uint32_t (&ok)[R],
                                           const uint64_t (&xv)[R][MAXV], int v, const unsigned (&peers)[R])
 {
+  // the caller rotates its preloaded values: this column's are element 0
+  (void)v;
   uint64_t x[R];
 #pragma unroll
-  for (int j = 0; j < R; ++j) {
-    x[j] = 0;
-#pragma unroll
-    for (int u = 0; u < MAXV; ++u)
-      if (u == v) x[j] = xv[j][u];
-  }
+  for (int j = 0; j < R; ++j) x[j] = xv[j][0];
   const int so = c.sum_off, mo = c.min_off, xo = c.max_off, qo = c.sq_off;
   const bool sum32 = c.sum_op == OP_SUM_I32;
   bool grouped[R];
@@ -860,9 +859,10 @@ __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant_
         }
       }
       load_keys(r0 + STEP, k0, k1, vb);
-      // one copy of the per-type column code, looped over the columns (the
-      // values are picked from registers by predicated moves), keeps the
-      // kernel small enough for the instruction cache
+      // one copy of the per-type column code, looped over the columns (each
+      // column's preloaded values are rotated into element 0 of the register
+      // array after the previous column), keeps the kernel small enough for
+      // the instruction cache
 #pragma unroll 1
       for (int v = 0; v < MAXV; ++v) {
         if (v >= nv) break;
@@ -892,6 +892,12 @@ __global__ void __launch_bounds__(NT, 1) k_part_aggregate(const __grid_constant_
           case (CAT_UNSIGNED << 4) | 2: p2_column<CAT_UNSIGNED, 2, R, MAXV, WAGG>(c, sa, ok, xv, v, peers); break;
           case (CAT_UNSIGNED << 4) | 1: p2_column<CAT_UNSIGNED, 1, R, MAXV, WAGG>(c, sa, ok, xv, v, peers); break;
           default: p2_column<CAT_BOOL, 1, R, MAXV, WAGG>(c, sa, ok, xv, v, peers); break;
+        }
+        // next column's values to element 0 (register moves, no indexed selection)
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+#pragma unroll
+          for (int u = 0; u + 1 < MAXV; ++u) xv[j][u] = xv[j][u + 1];
         }
       }
     }
