@@ -8,9 +8,11 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <set>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "gb_engine.h"
@@ -469,6 +471,17 @@ uint32_t* pinned()
   if (!t_pinned) ck(cudaMallocHost((void**)&t_pinned, kPinnedWords * 4), "cudaMallocHost");
   return t_pinned;
 }
+// Pinned staging of the partitioned path's region table (starts, ends,
+// cursors: 3 x 8 bytes for up to 8192 partitions), per host thread.  A call
+// finishes with a stream synchronisation, so the copy out of it is done before
+// the thread's next call writes it again.
+thread_local int64_t* t_regions = nullptr;
+constexpr size_t kRegionWords = 3 * 8192;
+int64_t* pinned_regions()
+{
+  if (!t_regions) ck(cudaMallocHost((void**)&t_regions, kRegionWords * 8), "cudaMallocHost");
+  return t_regions;
+}
 
 // HyperLogLog cardinality from 2^kHllBits registers (Flajolet et al. 2007):
 // E = alpha_m m^2 / sum 2^-M[j], with linear counting m ln(m/V) while E is
@@ -511,8 +524,26 @@ OutColumn make_out(const Allocator& A, cudaStream_t s, int type_id, int64_t rows
 int grid_for(const void* kernel, int block, size_t smem, int bps_cap)
 {
   DevInfo d = dev_info();
+  // the occupancy of a (kernel, block, shared memory) launch does not change
+  // once allow_max_smem has raised the kernel's limit: ask the runtime once
+  // per device and launch shape
+  static std::mutex mu;
+  static std::map<std::tuple<int, const void*, int, size_t>, int> memo;
+  int dev = 0;
+  ck(cudaGetDevice(&dev), "cudaGetDevice");
+  const auto key = std::make_tuple(dev, kernel, block, smem);
   int bps = 0;
-  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, block, smem), "occupancy");
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = memo.find(key);
+    if (it != memo.end()) bps = it->second;
+  }
+  if (bps == 0) {
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, block, smem), "occupancy");
+    if (bps < 1) bps = 1;
+    std::lock_guard<std::mutex> lk(mu);
+    memo[key] = bps;
+  }
   if (bps < 1) bps = 1;
   if (bps_cap > 0) bps = std::min(bps, bps_cap);
   return d.sms * bps;
@@ -789,12 +820,19 @@ Result aggregate(const std::vector<Column>& keys, int null_policy, const std::ve
   if (mode == 2) {
     // ---- pass 1: scatter rows into hash partitions ----
     int64_t total = pend.back();
-    int64_t* d_base = (int64_t*)S.get(sizeof(int64_t) * nparts);
-    int64_t* d_end = (int64_t*)S.get(sizeof(int64_t) * nparts);
-    unsigned long long* d_cur = (unsigned long long*)S.get(sizeof(unsigned long long) * nparts);
-    ck(cudaMemcpyAsync(d_base, pbase.data(), 8 * nparts, cudaMemcpyHostToDevice, stream), "h2d");
-    ck(cudaMemcpyAsync(d_end, pend.data(), 8 * nparts, cudaMemcpyHostToDevice, stream), "h2d");
-    ck(cudaMemcpyAsync(d_cur, pbase.data(), 8 * nparts, cudaMemcpyHostToDevice, stream), "h2d");
+    // region starts, ends and cursors (= starts): one pinned staging copy
+    // into one device block
+    int64_t* d_base = (int64_t*)S.get(3 * sizeof(int64_t) * nparts);
+    int64_t* d_end = d_base + nparts;
+    unsigned long long* d_cur = (unsigned long long*)(d_end + nparts);
+    {
+      if ((size_t)3 * nparts > kRegionWords) throw Error(ERR_LOGIC, "internal error: too many partitions");
+      int64_t* st3 = pinned_regions();
+      std::memcpy(st3, pbase.data(), 8 * nparts);
+      std::memcpy(st3 + nparts, pend.data(), 8 * nparts);
+      std::memcpy(st3 + 2 * nparts, pbase.data(), 8 * nparts);
+      ck(cudaMemcpyAsync(d_base, st3, 24 * (size_t)nparts, cudaMemcpyHostToDevice, stream), "h2d");
+    }
     PartArgs A;
     std::memset(&A, 0, sizeof(A));
     A.nparts = nparts;
