@@ -336,8 +336,12 @@ inline size_t part_scatter_smem(int kw, int tile, int nparts)
   return (size_t)tile * 8 + (size_t)tile * 2 + (size_t)nparts * 8 + 8 + (size_t)nparts * 8;
 }
 
-// Shared-memory find-or-insert (bounded probes); null when the key does not
-// fit (table at its fill limit or too many probes) or is the all-ones key.
+// Shared-memory find-or-insert; null when the key does not fit (table at its
+// fill limit) or is the all-ones key.  Probes take two slots per step for the
+// first 64 slots, then continue one slot at a time up to the table size: at
+// ~70% fill linear probing's longest runs in a table of a few thousand slots
+// pass 64, and a key cut off there would send all its rows of the item to the
+// spill list.
 // The table has `scap` slots, any count: the start slot is the low 32 hash
 // bits scaled to [0, scap) (multiply-shift), so the table can fill all the
 // shared memory a CTA has instead of the largest power of two below it.
@@ -381,6 +385,19 @@ __device__ __forceinline__ uint8_t* smem_slot(uint8_t* smem, int stride, uint32_
       }
       i = i1 + 1 == scap ? 0 : i1 + 1;
     }
+    // a run longer than 64 slots (a table near its fill limit): keep walking
+    // one slot at a time; below the fill limit an empty slot is always ahead
+    for (uint32_t p = 64; p < scap; ++p) {
+      unsigned long long* kp = (unsigned long long*)(smem + (size_t)i * stride);
+      const uint64_t c = *(volatile unsigned long long*)kp;
+      if (c == w0) return (uint8_t*)kp;
+      if (c == kEmpty) {
+        const int r = claim(kp);
+        if (r > 0) return (uint8_t*)kp;
+        if (r < 0) return nullptr;
+      }
+      i = i + 1 == scap ? 0 : i + 1;
+    }
     return nullptr;
   }
   // two-word keys: an empty slot has the top bit of its second word set
@@ -415,6 +432,14 @@ __device__ __forceinline__ uint8_t* smem_slot(uint8_t* smem, int stride, uint32_
     if (r > 0) return (uint8_t*)kp1;
     if (r < 0) return nullptr;
     i = i1 + 1 == scap ? 0 : i1 + 1;
+  }
+  // longer runs: one slot at a time, as for one-word keys
+  for (uint32_t p = 64; p < scap; ++p) {
+    unsigned __int128* kp = (unsigned __int128*)(smem + (size_t)i * stride);
+    const int r = look(kp, vload2(kp));
+    if (r > 0) return (uint8_t*)kp;
+    if (r < 0) return nullptr;
+    i = i + 1 == scap ? 0 : i + 1;
   }
   return nullptr;
 }
